@@ -1,0 +1,172 @@
+/*
+ * sph.h -- C ABI of the B200 SPH + FMM step (libsph_b200.so).
+ *
+ * Drop-in for the reference's pass API, class Compute
+ * (SPH/Compute/Compute.hpp:40-59).  A context owns every device buffer of one
+ * simulation; each pass is stream-ordered and asynchronous, like the
+ * reference's encoders into a caller-owned MTL::CommandBuffer, and the caller
+ * synchronises (sph_synchronize) where the reference commits and waits
+ * (SPH/Rendering/Headless.cpp:53-54).
+ *
+ * Plain types only: no CUDA or torch types cross this boundary.  A stream is
+ * passed as `void*` holding a cudaStream_t (NULL = the legacy default stream).
+ * Every call returns an sph_status; no exception crosses the ABI.  A context
+ * is used by one host thread at a time.
+ */
+#ifndef SPH_B200_H
+#define SPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SPH_OK = 0,
+    SPH_ERR_INVALID_ARG = 1,
+    SPH_ERR_OOM = 2,
+    SPH_ERR_IO = 3,
+    SPH_ERR_CUDA = 4,
+    SPH_ERR_DEVICE_HEALTH = 5, /* a kernel raised a health bit (see SPH_HEALTH_*) */
+    SPH_ERR_TIMEOUT = 6,       /* a bounded device wait gave up */
+    SPH_ERR_UNSUPPORTED = 7
+} sph_status;
+
+/* Health bits raised by kernels instead of trapping (sph_get_health). */
+#define SPH_HEALTH_SORT_TIMEOUT      0x0001u /* radix-sort look-back wait gave up */
+#define SPH_HEALTH_LIST_CAPACITY     0x0002u /* a tree level exceeded the unchecked-list storage */
+#define SPH_HEALTH_TREE_CAPACITY     0x0004u /* the tree outgrew its preallocated storage */
+#define SPH_HEALTH_NAN_DENSITY       0x0008u /* a density or pressure came out non-finite */
+#define SPH_HEALTH_SCAN_TIMEOUT      0x0010u /* a scan look-back wait gave up */
+#define SPH_HEALTH_ROOT_LEAF         0x0020u /* the root is a leaf: gravity pass skipped */
+
+typedef struct sph_ctx sph_ctx;
+
+/* Tree sources for the gravity pass. */
+#define SPH_TREE_GPU  0 /* Morton octree built on the GPU from sorted keys every sph_update_tree */
+#define SPH_TREE_HOST 1 /* a host-built tree in the reference format, given by sph_set_tree */
+
+/* Runtime knobs.  The physics constants of SPH/Parameters.h:11-53 are
+ * compiled into the kernels; these are the structural ones. */
+typedef struct {
+    int32_t max_children_in_leaf;   /* MAX_CHILDREN_IN_LEAF (Parameters.h:43), default 4 */
+    int32_t max_tree_depth;         /* MAX_TREE_DEPTH (Parameters.h:39), default 7, 1..10 */
+    int32_t max_unchecked_pointers; /* MAX_UNCHECKED_POINTERS (Parameters.h:42), default 1024 */
+    int32_t aneos_resolution;       /* ANEOS_TEXTURE_RESOLUTION (Parameters.h:20), default 2048 */
+    int32_t tree_source;            /* SPH_TREE_GPU (default) or SPH_TREE_HOST */
+    const char *forsterite_table;   /* ANEOS text table for material 400 (Compute.cpp:45) */
+    const char *fe85si15_table;     /* ANEOS text table for every other material (Compute.cpp:46) */
+} sph_params;
+
+/* Initial conditions: the fields of DataStruct that Compute loads
+ * (SPH/hdfHandler/hdfHandler.hpp:15-26, Compute.cpp:52-77).  Host pointers. */
+typedef struct {
+    int32_t n;
+    const float *pos;        /* 3n, xyz interleaved */
+    const float *vel;        /* 3n */
+    const float *rho;        /* n */
+    const float *u;          /* n, specific internal energy */
+    const float *mass;       /* n */
+    const float *pressure;   /* n */
+    const float *h;          /* n, smoothing length */
+    const int32_t *material; /* n, ANEOS material id (400 forsterite) */
+} sph_ic;
+
+/* Per-particle and global fields (sph_upload / sph_download / sph_get_buffer).
+ * Host-side element types: F3 = 3 floats per particle, F = float, I = int32,
+ * U = uint32, B = uint8.  Per-particle fields are in the original particle
+ * order.  CELL_* are the sorted cell arrays of Compute::sort. */
+typedef enum {
+    SPH_FIELD_POS = 0,          /* F3  positionBuffer */
+    SPH_FIELD_VEL = 1,          /* F3  _velocityBuffer */
+    SPH_FIELD_ACC = 2,          /* F3  _accelerationBuffer */
+    SPH_FIELD_RHO = 3,          /* F   densityBuffer */
+    SPH_FIELD_U = 4,            /* F   _internalEnergyBuffer */
+    SPH_FIELD_MASS = 5,         /* F   _massBuffer */
+    SPH_FIELD_PRESSURE = 6,     /* F   _pressureBuffer */
+    SPH_FIELD_H = 7,            /* F   _smoothingLengthBuffer */
+    SPH_FIELD_GRAD_TERM = 8,    /* F   _gradientTermsBuffer */
+    SPH_FIELD_SOUND_SPEED = 9,  /* F   _speedOfSoundBuffer */
+    SPH_FIELD_DU = 10,          /* F   _dInternalEnergyBuffer */
+    SPH_FIELD_BALSARA = 11,     /* F   _balsara */
+    SPH_FIELD_DHDT = 12,        /* F   _dhdt */
+    SPH_FIELD_GRAV_NORM = 13,   /* F   _gravAbs */
+    SPH_FIELD_MATERIAL = 14,    /* I   materialIdBuffer */
+    SPH_FIELD_ACTIVE = 15,      /* B   _active */
+    SPH_FIELD_NEXT_ACTIVE = 16, /* I   _nextActiveTime */
+    SPH_FIELD_GLOBAL_TIME = 17, /* I   _globalTime (1 value, ticks of 32/65536 s) */
+    SPH_FIELD_DT = 18,          /* I   _dt (1 value, ticks) */
+    SPH_FIELD_CELL_KEY = 19,    /* U   _cellArrayi[].x after sort (n) */
+    SPH_FIELD_CELL_INDEX = 20,  /* U   _cellArrayi[].y after sort (n) */
+    SPH_FIELD_CELL_START = 21,  /* U   _cellStart (2^24), UINT_MAX when empty; download only */
+    SPH_FIELD_CELL_END = 22,    /* U   _cellEnd (2^24), 0 when empty; download only */
+    SPH_FIELD_COUNT = 23
+} sph_field;
+
+/* Defaults equal to SPH/Parameters.h (table paths are the reference's names). */
+void sph_params_default(sph_params *p);
+
+/* Compute::Compute (Compute.cpp:22-36, 44-132): allocate, load the two EOS
+ * tables, upload the initial state (active = 1, nextActiveTime = 0, time = 0),
+ * select the current CUDA device.  For SPH_TREE_GPU the first tree is built
+ * here; for SPH_TREE_HOST call sph_set_tree before sph_gravity. */
+sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out);
+sph_status sph_destroy(sph_ctx *ctx);
+int32_t sph_num_particles(const sph_ctx *ctx);
+
+/* Compute::updateOctreeBuffer (Compute.cpp:456-508): rebuild the octree on the
+ * GPU from the current positions (SPH_TREE_GPU).  No host thread. */
+sph_status sph_update_tree(sph_ctx *ctx, void *stream);
+/* Give the context a tree in the reference's flattened format (octree.cpp:24-109):
+ * leaf [n, dataPtr, p0..], branch [0, dataPtr, c0..c7 or -1]; levels as node
+ * offsets (level_offsets has n_levels+1 entries into level_nodes). */
+sph_status sph_set_tree(sph_ctx *ctx, const int32_t *tree, int32_t tree_len, const int32_t *level_offsets,
+                        const int32_t *level_nodes, int32_t n_levels, int32_t n_nodes);
+
+/* Read back the current tree (synchronous).  Any output pointer may be NULL to
+ * query sizes only; level_offsets needs room for 17 entries. */
+sph_status sph_get_tree(sph_ctx *ctx, int32_t *tree, int64_t tree_room, int32_t *tree_len, int32_t *level_offsets,
+                        int32_t *level_nodes, int64_t level_nodes_room, int32_t *n_levels, int32_t *n_nodes);
+
+/* The passes of Headless::step (Headless.cpp:43-51), in order. */
+sph_status sph_sort(sph_ctx *ctx, void *stream);         /* Compute::sort (Compute.cpp:265-326) */
+sph_status sph_gravity(sph_ctx *ctx, void *stream);      /* Compute::gravitationalPass (:328-377) */
+sph_status sph_density(sph_ctx *ctx, void *stream);      /* Compute::densityPass (:179-208) */
+sph_status sph_acceleration(sph_ctx *ctx, void *stream); /* Compute::accelerationPass (:210-240) */
+sph_status sph_step(sph_ctx *ctx, void *stream);         /* Compute::stepPass (:242-263) */
+
+/* n_steps x (tree, sort, gravity, density, acceleration, step), replayed from
+ * a CUDA graph captured on first use (Headless::step without the snapshot). */
+sph_status sph_step_all(sph_ctx *ctx, void *stream, int32_t n_steps);
+
+/* Compute::drawSnapshot (Compute.cpp:396-448, render.metal:49-66): splat the
+ * material ids into a 1024x1024 int image by atomic max.  When image is not
+ * NULL it receives the image (synchronous). */
+sph_status sph_draw_snapshot(sph_ctx *ctx, void *stream, int32_t *image);
+
+/* Buffers.hpp:14-59 (writeDataToPrivateBuffer): synchronous host<->device copies.
+ * count = number of host elements (3n floats for F3 fields, n otherwise). */
+sph_status sph_upload(sph_ctx *ctx, sph_field field, const void *host, size_t count);
+sph_status sph_download(sph_ctx *ctx, sph_field field, void *host, size_t count);
+/* Borrow the device buffer behind a field (valid until sph_destroy).  F3 fields
+ * are stored as 16-byte float4 records; the reported stride is in *stride. */
+sph_status sph_get_buffer(sph_ctx *ctx, sph_field field, void **device_ptr, size_t *bytes, size_t *stride);
+
+/* Wait for the stream, then report SPH_ERR_DEVICE_HEALTH if a health bit is set. */
+sph_status sph_synchronize(sph_ctx *ctx, void *stream);
+sph_status sph_get_health(sph_ctx *ctx, uint32_t *word);
+sph_status sph_clear_health(sph_ctx *ctx);
+
+/* Host-only helpers (no GPU work). */
+/* ANEOS.cpp:21-175: parse a table and resample it to res x res (pressure,
+ * sound speed) pairs, rho rows, u columns.  out holds 2*res*res floats. */
+sph_status sph_eos_resample(const char *path, int32_t res, float *out);
+const char *sph_status_string(sph_status s);
+const char *sph_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPH_B200_H */

@@ -1,0 +1,274 @@
+"""ctypes harness for the CPU oracle (liboracle.so) and, when built, the
+reference's own kernels compiled on the host (_ref/libref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, never by the product package.
+
+Both libraries take the same `ora_state` (oracle.h): SoA arrays in original
+particle order, xyz-interleaved vectors.  `OracleState` owns the numpy arrays
+and exposes the pass API in the reference's order (sort, gravity, density,
+acceleration, step).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libref.so")
+NCELLS = 1 << 24
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_up = C.POINTER(C.c_uint32)
+_bp = C.POINTER(C.c_uint8)
+
+
+class OraState(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32),
+        ("pos", _fp), ("vel", _fp), ("acc", _fp),
+        ("rho", _fp), ("u", _fp), ("mass", _fp), ("pressure", _fp), ("h", _fp),
+        ("grad_term", _fp), ("sound_speed", _fp), ("du", _fp), ("balsara", _fp), ("dhdt", _fp),
+        ("grav_norm", _fp),
+        ("material", _ip), ("active", _bp), ("next_active_time", _ip),
+        ("global_time", _ip), ("dt", _ip),
+        ("cell_key", _up), ("cell_index", _up), ("cell_start", _up), ("cell_end", _up),
+        ("eos_forsterite", _fp), ("eos_fe", _fp), ("eos_res", C.c_int32),
+        ("tree", _ip), ("tree_len", C.c_int32), ("level_offsets", _ip), ("level_nodes", _ip),
+        ("n_levels", C.c_int32), ("n_nodes", C.c_int32), ("max_unchecked", C.c_int32),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the system g++ (OpenMP, no FP contraction)."""
+    src = os.path.join(HERE, "oracle.cpp")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        cxx = os.environ.get("SPH_HOST_CXX", "g++")
+        cmd = [cxx, "-O3", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
+               "-fno-fast-math", "-o", LIB_PATH + ".tmp", src]
+        subprocess.run(cmd, check=True)
+        os.replace(LIB_PATH + ".tmp", LIB_PATH)
+    return LIB_PATH
+
+
+def build_ref(reference_root: str = "/root/reference") -> str | None:
+    """Build _ref/libref.so from the reference's sources when they are present."""
+    if not os.path.isdir(os.path.join(reference_root, "SPH", "Shaders")):
+        return None
+    subprocess.run([os.path.join(HERE, "ref_build.sh"), reference_root], check=True,
+                   stdout=subprocess.DEVNULL)
+    return REF_PATH
+
+
+def _bind(lib: C.CDLL, prefix: str) -> C.CDLL:
+    st = C.POINTER(OraState)
+    for name in ("sort", "gravity", "density", "acceleration", "step"):
+        f = getattr(lib, f"{prefix}_{name}")
+        f.argtypes = [st]
+        f.restype = None
+    return lib
+
+
+_LIBS: dict = {}
+
+
+def load(kind: str = "oracle") -> C.CDLL:
+    """kind 'oracle' (restatement) or 'ref' (reference kernels via the shim)."""
+    if kind in _LIBS:
+        return _LIBS[kind]
+    if kind == "oracle":
+        lib = C.CDLL(build())
+        _bind(lib, "ora")
+        vp = C.c_void_p
+        for fn in ("ora_tree_build_reference", "ora_tree_build_morton"):
+            getattr(lib, fn).argtypes = [C.c_int, _fp, C.c_int, C.c_int]
+            getattr(lib, fn).restype = vp
+        lib.ora_tree_sizes.argtypes = [vp, _ip, _ip, _ip]
+        lib.ora_tree_export.argtypes = [vp, _ip, _ip, _ip]
+        lib.ora_tree_free.argtypes = [vp]
+        lib.ora_aneos_load.argtypes = [C.c_char_p, C.c_int, _fp]
+        lib.ora_aneos_load.restype = C.c_int
+        lib.ora_cell_key.argtypes = [C.c_float, C.c_float, C.c_float]
+        lib.ora_cell_key.restype = C.c_uint32
+        lib.ora_set_threads.argtypes = [C.c_int]
+        lib.ora_get_threads.restype = C.c_int
+    elif kind == "ref":
+        if not os.path.exists(REF_PATH):
+            raise FileNotFoundError(REF_PATH)
+        lib = C.CDLL(REF_PATH)
+        _bind(lib, "ref")
+        vp = C.c_void_p
+        lib.ref_tree_build.argtypes = [C.c_int, _fp, C.c_int]
+        lib.ref_tree_build.restype = vp
+        lib.ref_tree_sizes.argtypes = [vp, _ip, _ip, _ip]
+        lib.ref_tree_export.argtypes = [vp, _ip, _ip, _ip]
+        lib.ref_tree_free.argtypes = [vp]
+        lib.ref_aneos_load.argtypes = [C.c_char_p, C.c_int, _fp]
+        lib.ref_aneos_load.restype = C.c_int
+    else:
+        raise ValueError(kind)
+    _LIBS[kind] = lib
+    return lib
+
+
+def ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+def _export_tree(lib, prefix: str, handle) -> dict:
+    ln, nl, nn = C.c_int32(), C.c_int32(), C.c_int32()
+    getattr(lib, f"{prefix}_tree_sizes")(handle, C.byref(ln), C.byref(nl), C.byref(nn))
+    tree = np.zeros(max(ln.value, 1), np.int32)
+    off = np.zeros(nl.value + 1, np.int32)
+    nodes = np.zeros(max(ln.value, 1), np.int32)
+    getattr(lib, f"{prefix}_tree_export")(handle, ptr(tree, _ip), ptr(off, _ip), ptr(nodes, _ip))
+    getattr(lib, f"{prefix}_tree_free")(handle)
+    return dict(tree=tree[:ln.value], level_offsets=off, level_nodes=nodes[:off[-1]],
+                n_levels=nl.value, n_nodes=nn.value)
+
+
+def tree_reference(pos: np.ndarray, max_leaf: int, max_depth: int = 7, kind: str = "oracle") -> dict:
+    """The reference's mean-split CPU octree (octree.cpp), from the oracle
+    restatement or from the reference file itself (kind='ref', depth fixed 7)."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    lib = load(kind)
+    if kind == "ref":
+        h = lib.ref_tree_build(pos.shape[0], ptr(pos, _fp), max_leaf)
+        return _export_tree(lib, "ref", h)
+    h = lib.ora_tree_build_reference(pos.shape[0], ptr(pos, _fp), max_leaf, max_depth)
+    return _export_tree(lib, "ora", h)
+
+
+def tree_morton(pos: np.ndarray, max_leaf: int, max_depth: int = 7) -> dict:
+    """The GPU builder's Morton octree, restated on the CPU."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    lib = load("oracle")
+    h = lib.ora_tree_build_morton(pos.shape[0], ptr(pos, _fp), max_leaf, max_depth)
+    return _export_tree(lib, "ora", h)
+
+
+def aneos_load(path: str, res: int = 2048, kind: str = "oracle") -> np.ndarray:
+    out = np.zeros((res, res, 2), np.float32)
+    lib = load(kind)
+    fn = lib.ora_aneos_load if kind == "oracle" else lib.ref_aneos_load
+    rc = fn(path.encode(), res, ptr(out, _fp))
+    if rc != 0:
+        raise RuntimeError(f"ANEOS load failed ({rc}) for {path}")
+    return out
+
+
+FLOAT_FIELDS = ("rho", "u", "mass", "pressure", "h", "grad_term", "sound_speed", "du", "balsara",
+                "dhdt", "grav_norm")
+
+
+class OracleState:
+    """Owns one simulation's arrays; passes run through liboracle or libref."""
+
+    def __init__(self, ic: dict, eos_forsterite: np.ndarray, eos_fe: np.ndarray, kind: str = "oracle",
+                 max_unchecked: int = 1024):
+        n = int(ic["pos"].shape[0])
+        self.n = n
+        self.kind = kind
+        self.lib = load(kind)
+        self.prefix = "ora" if kind == "oracle" else "ref"
+        f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+        self.pos = f32(ic["pos"]).reshape(n, 3).copy()
+        self.vel = f32(ic["vel"]).reshape(n, 3).copy()
+        self.acc = np.zeros((n, 3), np.float32)
+        self.rho = f32(ic["rho"]).copy()
+        self.u = f32(ic["u"]).copy()
+        self.mass = f32(ic["mass"]).copy()
+        self.pressure = f32(ic.get("pressure", np.zeros(n))).copy()
+        self.h = f32(ic["h"]).copy()
+        for name in ("grad_term", "sound_speed", "du", "balsara", "dhdt", "grav_norm"):
+            setattr(self, name, np.zeros(n, np.float32))
+        self.material = np.ascontiguousarray(ic["material"], dtype=np.int32).copy()
+        self.active = np.ones(n, np.uint8)                 # Compute.cpp:66-70
+        self.next_active_time = np.zeros(n, np.int32)      # Compute.cpp:73-77
+        self.global_time = np.zeros(1, np.int32)
+        self.dt = np.zeros(1, np.int32)
+        self.cell_key = np.zeros(n, np.uint32)
+        self.cell_index = np.zeros(n, np.uint32)
+        self.cell_start = np.zeros(NCELLS, np.uint32)
+        self.cell_end = np.zeros(NCELLS, np.uint32)
+        self.eos_forsterite = f32(eos_forsterite)
+        self.eos_fe = f32(eos_fe)
+        self.eos_res = int(eos_forsterite.shape[0])
+        self.max_unchecked = max_unchecked
+        self.tree = None
+        self._st = OraState()
+        self._fill()
+
+    def _fill(self):
+        s = self._st
+        s.n = self.n
+        for name in ("pos", "vel", "acc") + FLOAT_FIELDS:
+            setattr(s, name, ptr(getattr(self, name), _fp))
+        s.material = ptr(self.material, _ip)
+        s.active = ptr(self.active, _bp)
+        s.next_active_time = ptr(self.next_active_time, _ip)
+        s.global_time = ptr(self.global_time, _ip)
+        s.dt = ptr(self.dt, _ip)
+        for name in ("cell_key", "cell_index", "cell_start", "cell_end"):
+            setattr(s, name, ptr(getattr(self, name), _up))
+        s.eos_forsterite = ptr(self.eos_forsterite, _fp)
+        s.eos_fe = ptr(self.eos_fe, _fp)
+        s.eos_res = self.eos_res
+        s.max_unchecked = self.max_unchecked
+        if self.tree is not None:
+            t = self.tree
+            s.tree = ptr(t["tree"], _ip)
+            s.tree_len = int(t["tree"].shape[0])
+            s.level_offsets = ptr(t["level_offsets"], _ip)
+            s.level_nodes = ptr(t["level_nodes"], _ip)
+            s.n_levels = int(t["n_levels"])
+            s.n_nodes = int(t["n_nodes"])
+        else:
+            s.n_levels = 0
+            s.tree_len = 0
+            s.n_nodes = 0
+
+    def set_tree(self, tree: dict):
+        self.tree = {k: (np.ascontiguousarray(v, np.int32) if isinstance(v, np.ndarray) else v)
+                     for k, v in tree.items()}
+        self._fill()
+
+    def _call(self, name):
+        getattr(self.lib, f"{self.prefix}_{name}")(C.byref(self._st))
+
+    def sort(self):
+        self._call("sort")
+
+    def gravity(self):
+        self._call("gravity")
+
+    def density(self):
+        self._call("density")
+
+    def acceleration(self):
+        self._call("acceleration")
+
+    def step(self):
+        self._call("step")
+
+    def full_step(self, tree_fn=None):
+        """One global step in the reference's order (Headless.cpp:43-51), with
+        the tree rebuilt from the current positions by `tree_fn` first."""
+        if tree_fn is not None:
+            self.set_tree(tree_fn(self.pos))
+        self.sort()
+        self.gravity()
+        self.density()
+        self.acceleration()
+        self.step()
+
+    def snapshot(self) -> dict:
+        out = {k: getattr(self, k).copy() for k in ("pos", "vel", "acc") + FLOAT_FIELDS}
+        for k in ("material", "active", "next_active_time", "global_time", "dt", "cell_key", "cell_index"):
+            out[k] = getattr(self, k).copy()
+        return out

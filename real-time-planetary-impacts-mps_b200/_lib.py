@@ -1,0 +1,148 @@
+"""ctypes binding of libsph_b200.so (include/sph.h) and its in-tree build.
+
+The library is built in place (nvcc, sm_100a) next to this file so that it
+travels with the repository; `load()` fails loudly when it is missing or when
+no CUDA device is visible -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libsph_b200.so")
+SOURCES = ["sph_api.cu", "sph_sort.cu", "sph_hydro.cu", "sph_gravity.cu", "sph_tree.cu"]
+HEADERS = ["sph_common.cuh", "sph_internal.h"]
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+              "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared"]
+
+SPH_OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "i/o error", 4: "cuda error",
+          5: "device health bit raised", 6: "bounded device wait timed out", 7: "unsupported"}
+
+SPH_TREE_GPU = 0
+SPH_TREE_HOST = 1
+
+FIELDS = {
+    "pos": 0, "vel": 1, "acc": 2, "rho": 3, "u": 4, "mass": 5, "pressure": 6, "h": 7,
+    "grad_term": 8, "sound_speed": 9, "du": 10, "balsara": 11, "dhdt": 12, "grav_norm": 13,
+    "material": 14, "active": 15, "next_active_time": 16, "global_time": 17, "dt": 18,
+    "cell_key": 19, "cell_index": 20, "cell_start": 21, "cell_end": 22,
+}
+VECTOR_FIELDS = ("pos", "vel", "acc")
+
+HEALTH = {"sort_timeout": 0x1, "list_capacity": 0x2, "tree_capacity": 0x4, "nan_density": 0x8,
+          "scan_timeout": 0x10, "root_leaf": 0x20}
+
+
+class SphParams(C.Structure):
+    _fields_ = [
+        ("max_children_in_leaf", C.c_int32),
+        ("max_tree_depth", C.c_int32),
+        ("max_unchecked_pointers", C.c_int32),
+        ("aneos_resolution", C.c_int32),
+        ("tree_source", C.c_int32),
+        ("forsterite_table", C.c_char_p),
+        ("fe85si15_table", C.c_char_p),
+    ]
+
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+
+
+class SphIC(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32),
+        ("pos", _fp), ("vel", _fp), ("rho", _fp), ("u", _fp), ("mass", _fp), ("pressure", _fp), ("h", _fp),
+        ("material", _ip),
+    ]
+
+
+class SphError(RuntimeError):
+    def __init__(self, status: int, what: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, status)}" + (f" ({detail})" if detail else ""))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile libsph_b200.so for sm_100a in place (cross-compiles without a GPU)."""
+    csrc = os.path.join(HERE, "csrc")
+    srcs = [os.path.join(csrc, s) for s in SOURCES]
+    deps = srcs + [os.path.join(csrc, h) for h in HEADERS] + [os.path.join(ROOT, "include", "sph.h")]
+    if not force and os.path.exists(LIB_PATH):
+        t = os.path.getmtime(LIB_PATH)
+        if all(os.path.getmtime(d) <= t for d in deps):
+            return LIB_PATH
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    if not os.path.exists(nvcc):
+        nvcc = "nvcc"
+    tmp = LIB_PATH + f".{os.getpid()}.tmp"
+    cmd = [nvcc] + NVCC_FLAGS + ["-o", tmp] + srcs
+    res = subprocess.run(cmd, capture_output=not verbose, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + (res.stderr or "") + (res.stdout or ""))
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def load() -> C.CDLL:
+    """Load the CUDA library (built in place).  Raises if it is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is not built; run __graft_entry__.build()")
+    lib = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    st = C.c_int
+    sig = {
+        "sph_params_default": (None, [C.POINTER(SphParams)]),
+        "sph_create": (st, [C.POINTER(SphParams), C.POINTER(SphIC), C.POINTER(vp)]),
+        "sph_destroy": (st, [vp]),
+        "sph_num_particles": (C.c_int32, [vp]),
+        "sph_update_tree": (st, [vp, vp]),
+        "sph_get_tree": (st, [vp, _ip, C.c_int64, _ip, _ip, _ip, C.c_int64, _ip, _ip]),
+        "sph_set_tree": (st, [vp, _ip, C.c_int32, _ip, _ip, C.c_int32, C.c_int32]),
+        "sph_sort": (st, [vp, vp]),
+        "sph_gravity": (st, [vp, vp]),
+        "sph_density": (st, [vp, vp]),
+        "sph_acceleration": (st, [vp, vp]),
+        "sph_step": (st, [vp, vp]),
+        "sph_step_all": (st, [vp, vp, C.c_int32]),
+        "sph_draw_snapshot": (st, [vp, vp, _ip]),
+        "sph_upload": (st, [vp, C.c_int, vp, C.c_size_t]),
+        "sph_download": (st, [vp, C.c_int, vp, C.c_size_t]),
+        "sph_get_buffer": (st, [vp, C.c_int, C.POINTER(vp), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+        "sph_synchronize": (st, [vp, vp]),
+        "sph_get_health": (st, [vp, C.POINTER(C.c_uint32)]),
+        "sph_clear_health": (st, [vp]),
+        "sph_eos_resample": (st, [C.c_char_p, C.c_int32, _fp]),
+        "sph_status_string": (C.c_char_p, [st]),
+        "sph_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def check(status: int, what: str):
+    if status != SPH_OK:
+        detail = load().sph_last_error().decode(errors="replace")
+        raise SphError(status, what, detail)
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/sph.h (for the export check)."""
+    import re
+    with open(os.path.join(ROOT, "include", "sph.h")) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(sph_[a-z0-9_]+)\s*\(", text)))

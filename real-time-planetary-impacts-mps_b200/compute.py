@@ -1,0 +1,242 @@
+"""Host-side mirror of the reference's pass API, class Compute
+(SPH/Compute/Compute.hpp:40-59), over the C ABI of libsph_b200.so.
+
+    Compute(ic, ...)        Compute::Compute (Compute.cpp:22-36)
+    updateOctreeBuffer()    Compute::updateOctreeBuffer (:456-508), GPU build
+    sort()                  Compute::sort (:265-326)
+    gravitationalPass()     Compute::gravitationalPass (:328-377)
+    densityPass()           Compute::densityPass (:179-208)
+    accelerationPass()      Compute::accelerationPass (:210-240)
+    stepPass()              Compute::stepPass (:242-263)
+    drawSnapshot()          Compute::drawSnapshot (:396-448)
+    positionBuffer, materialIdBuffer, densityBuffer, nParticles  (public members)
+
+Each pass takes an optional CUDA stream (an int cudaStream_t, or an object with
+a `cuda_stream` attribute such as torch.cuda.Stream) in place of the
+reference's MTL::CommandBuffer; passes are asynchronous until synchronize().
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _lib
+from . import eos_tables
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+
+
+def _stream(s) -> C.c_void_p:
+    if s is None:
+        return C.c_void_p(0)
+    if hasattr(s, "cuda_stream"):
+        return C.c_void_p(int(s.cuda_stream))
+    return C.c_void_p(int(s))
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+class Compute:
+    """One simulation on the current CUDA device."""
+
+    def __init__(self, ic: dict, *, max_children_in_leaf: int = 4, max_tree_depth: int = 7,
+                 max_unchecked_pointers: int = 1024, aneos_resolution: int = 2048,
+                 tree_source: str = "gpu", forsterite_table: str | None = None,
+                 fe85si15_table: str | None = None):
+        lib = _lib.load()
+        if forsterite_table is None or fe85si15_table is None:
+            tabs = eos_tables.ensure_tables()
+            forsterite_table = forsterite_table or tabs["forsterite"]
+            fe85si15_table = fe85si15_table or tabs["Fe85Si15"]
+        if not os.path.exists(forsterite_table) or not os.path.exists(fe85si15_table):
+            raise FileNotFoundError("ANEOS tables not found")
+        p = _lib.SphParams()
+        lib.sph_params_default(C.byref(p))
+        p.max_children_in_leaf = max_children_in_leaf
+        p.max_tree_depth = max_tree_depth
+        p.max_unchecked_pointers = max_unchecked_pointers
+        p.aneos_resolution = aneos_resolution
+        p.tree_source = _lib.SPH_TREE_GPU if tree_source == "gpu" else _lib.SPH_TREE_HOST
+        self._paths = (forsterite_table.encode(), fe85si15_table.encode())
+        p.forsterite_table = self._paths[0]
+        p.fe85si15_table = self._paths[1]
+        n = int(np.asarray(ic["pos"]).reshape(-1, 3).shape[0])
+        f32 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float32).reshape(-1))  # noqa: E731
+        keep = dict(pos=f32(ic["pos"]), vel=f32(ic["vel"]), rho=f32(ic["rho"]), u=f32(ic["u"]),
+                    mass=f32(ic["mass"]), pressure=f32(ic.get("pressure", np.zeros(n))), h=f32(ic["h"]),
+                    material=np.ascontiguousarray(np.asarray(ic["material"], dtype=np.int32).reshape(-1)))
+        s = _lib.SphIC()
+        s.n = n
+        for k in ("pos", "vel", "rho", "u", "mass", "pressure", "h"):
+            setattr(s, k, _ptr(keep[k], _fp))
+        s.material = _ptr(keep["material"], _ip)
+        h = C.c_void_p()
+        _lib.check(lib.sph_create(C.byref(p), C.byref(s), C.byref(h)), "sph_create")
+        self._lib = lib
+        self._h = h
+        self.nParticles = n
+        self.tree_source = tree_source
+
+    # ---- lifetime ------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.sph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- passes (Headless.cpp:43-51 order) -----------------------------
+    def updateOctreeBuffer(self, stream=None):
+        _lib.check(self._lib.sph_update_tree(self._h, _stream(stream)), "sph_update_tree")
+
+    def sort(self, stream=None):
+        _lib.check(self._lib.sph_sort(self._h, _stream(stream)), "sph_sort")
+
+    def gravitationalPass(self, stream=None):
+        _lib.check(self._lib.sph_gravity(self._h, _stream(stream)), "sph_gravity")
+
+    def densityPass(self, stream=None):
+        _lib.check(self._lib.sph_density(self._h, _stream(stream)), "sph_density")
+
+    def accelerationPass(self, stream=None):
+        _lib.check(self._lib.sph_acceleration(self._h, _stream(stream)), "sph_acceleration")
+
+    def stepPass(self, stream=None):
+        _lib.check(self._lib.sph_step(self._h, _stream(stream)), "sph_step")
+
+    def drawSnapshot(self, stream=None, download: bool = True):
+        if not download:
+            _lib.check(self._lib.sph_draw_snapshot(self._h, _stream(stream), None), "sph_draw_snapshot")
+            return None
+        img = np.zeros((1024, 1024), np.int32)
+        _lib.check(self._lib.sph_draw_snapshot(self._h, _stream(stream), _ptr(img, _ip)), "sph_draw_snapshot")
+        return img
+
+    def step(self, stream=None):
+        """One Headless::step without the snapshot: tree, sort, gravity,
+        density, acceleration, step."""
+        self.updateOctreeBuffer(stream)
+        self.sort(stream)
+        self.gravitationalPass(stream)
+        self.densityPass(stream)
+        self.accelerationPass(stream)
+        self.stepPass(stream)
+
+    def step_all(self, n_steps: int, stream=None):
+        """n_steps full steps replayed from a captured CUDA graph."""
+        _lib.check(self._lib.sph_step_all(self._h, _stream(stream), int(n_steps)), "sph_step_all")
+
+    def synchronize(self, stream=None):
+        _lib.check(self._lib.sph_synchronize(self._h, _stream(stream)), "sph_synchronize")
+
+    # ---- trees ---------------------------------------------------------
+    def set_tree(self, tree: dict):
+        """Give a host-built tree in the reference format (see oracle/oracle.py
+        tree_reference); later gravity passes use it until the next call."""
+        t = np.ascontiguousarray(tree["tree"], np.int32)
+        off = np.ascontiguousarray(tree["level_offsets"], np.int32)
+        nodes = np.ascontiguousarray(tree["level_nodes"], np.int32)
+        _lib.check(self._lib.sph_set_tree(self._h, _ptr(t, _ip), int(t.shape[0]), _ptr(off, _ip),
+                                          _ptr(nodes, _ip), int(tree["n_levels"]), int(tree["n_nodes"])),
+                   "sph_set_tree")
+        self.tree_source = "host"
+
+    def get_tree(self) -> dict:
+        """The current tree in the reference format (synchronous)."""
+        ln, nl, nn = C.c_int32(), C.c_int32(), C.c_int32()
+        _lib.check(self._lib.sph_get_tree(self._h, None, 0, C.byref(ln), None, None, 0, C.byref(nl), C.byref(nn)),
+                   "sph_get_tree")
+        tree = np.zeros(max(ln.value, 1), np.int32)
+        off = np.zeros(17, np.int32)
+        nodes = np.zeros(max(nn.value, 1), np.int32)
+        _lib.check(self._lib.sph_get_tree(self._h, _ptr(tree, _ip), tree.size, C.byref(ln), _ptr(off, _ip),
+                                          _ptr(nodes, _ip), nodes.size, C.byref(nl), C.byref(nn)), "sph_get_tree")
+        return dict(tree=tree[:ln.value], level_offsets=off[:nl.value + 1], level_nodes=nodes[:off[nl.value]],
+                    n_levels=nl.value, n_nodes=nn.value)
+
+    # ---- buffers (Buffers.hpp:14-59) -------------------------------------
+    def download(self, field: str) -> np.ndarray:
+        n = self.nParticles
+        if field in _lib.VECTOR_FIELDS:
+            out = np.zeros((n, 3), np.float32)
+        elif field in ("global_time", "dt"):
+            out = np.zeros(1, np.int32)
+        elif field in ("material", "next_active_time"):
+            out = np.zeros(n, np.int32)
+        elif field == "active":
+            out = np.zeros(n, np.uint8)
+        elif field in ("cell_key", "cell_index"):
+            out = np.zeros(n, np.uint32)
+        elif field in ("cell_start", "cell_end"):
+            out = np.zeros(1 << 24, np.uint32)
+        else:
+            out = np.zeros(n, np.float32)
+        _lib.check(self._lib.sph_download(self._h, _lib.FIELDS[field], out.ctypes.data_as(C.c_void_p), out.size),
+                   f"sph_download({field})")
+        return out
+
+    def upload(self, field: str, values) -> None:
+        if field in _lib.VECTOR_FIELDS:
+            a = np.ascontiguousarray(np.asarray(values, np.float32).reshape(-1))
+        elif field in ("global_time", "dt", "material", "next_active_time"):
+            a = np.ascontiguousarray(np.asarray(values, np.int32).reshape(-1))
+        elif field == "active":
+            a = np.ascontiguousarray(np.asarray(values, np.uint8).reshape(-1))
+        else:
+            a = np.ascontiguousarray(np.asarray(values, np.float32).reshape(-1))
+        _lib.check(self._lib.sph_upload(self._h, _lib.FIELDS[field], a.ctypes.data_as(C.c_void_p), a.size),
+                   f"sph_upload({field})")
+
+    def device_buffer(self, field: str):
+        """(device pointer, bytes, stride) of a field's storage."""
+        p, b, s = C.c_void_p(), C.c_size_t(), C.c_size_t()
+        _lib.check(self._lib.sph_get_buffer(self._h, _lib.FIELDS[field], C.byref(p), C.byref(b), C.byref(s)),
+                   "sph_get_buffer")
+        return p.value, b.value, s.value
+
+    @property
+    def positionBuffer(self):
+        return self.device_buffer("pos")
+
+    @property
+    def materialIdBuffer(self):
+        return self.device_buffer("material")
+
+    @property
+    def densityBuffer(self):
+        return self.device_buffer("rho")
+
+    def health(self) -> int:
+        w = C.c_uint32()
+        _lib.check(self._lib.sph_get_health(self._h, C.byref(w)), "sph_get_health")
+        return w.value
+
+    def clear_health(self):
+        _lib.check(self._lib.sph_clear_health(self._h), "sph_clear_health")
+
+    def state(self) -> dict:
+        names = ("pos", "vel", "acc", "rho", "u", "mass", "pressure", "h", "grad_term", "sound_speed", "du",
+                 "balsara", "dhdt", "grav_norm", "material", "active", "next_active_time", "global_time", "dt")
+        return {k: self.download(k) for k in names}
+
+
+def eos_resample(path: str, res: int = 2048) -> np.ndarray:
+    """The library's host-side ANEOS resampler (no GPU work)."""
+    out = np.zeros((res, res, 2), np.float32)
+    _lib.check(_lib.load().sph_eos_resample(path.encode(), res, _ptr(out, _fp)), "sph_eos_resample")
+    return out

@@ -1,0 +1,153 @@
+// sph_internal.h -- the context behind the C ABI and the launchers each .cu
+// file provides.  Device memory layout (all per-particle arrays in the
+// original particle order unless named s*):
+//
+//   pos4 (x, y, z, mass)  vel4 (vx, vy, vz, 0)  acc4 (ax, ay, az, 0)  float4
+//   rho u P h f c du B dhdt gnorm                                       float
+//   mat next_active                                                     int32
+//   active                                                              uint8
+//   globals[0] global time, globals[1] dt (ticks)                       int32
+//   cell_range[2^24] (first, last sorted index; UINT_MAX/0 when empty)  uint2
+//   sorted working set, index = sorted slot:
+//     sp4 (x, y, z, m)  sv4 (vx, vy, vz, 0)        gathered before density
+//     sA (x, y, z, h)   sB (vx, vy, vz, c)   sC (m, f P / rho^2, rho, B)
+//                                               written by density, read by acceleration
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/sph.h"
+#include "sph_common.cuh"
+
+namespace sph {
+
+// One-sweep LSD radix sorter for (uint32 key, uint32 value) pairs.
+struct RadixSorter {
+    uint32_t *keys[2] = {nullptr, nullptr};
+    uint32_t *vals[2] = {nullptr, nullptr};
+    uint32_t *hist = nullptr;     // [kMaxPasses][256] digit counts, filled by the key producer
+    uint32_t *status = nullptr;   // [kMaxPasses][tiles][256] look-back words
+    uint32_t *counters = nullptr; // [kMaxPasses] tile tickets
+    int n_cap = 0;
+    int tiles_cap = 0;
+    static constexpr int kThreads = 256;
+    static constexpr int kItems = 16;
+    static constexpr int kTile = kThreads * kItems;
+    static constexpr int kMaxPasses = 4;
+};
+
+// Device-resident octree in the reference's flattened format plus the node
+// records of the FMM passes.
+struct Tree {
+    int32_t *tree = nullptr;        // flattened ints
+    int64_t tree_cap = 0;
+    int32_t *level_nodes = nullptr; // [max_levels][level_cap] tree offsets, DFS order within a level
+    int32_t *level_count = nullptr; // [max_levels] (device)
+    int32_t *list_slot = nullptr;   // [node_cap] by data pointer: branch rank within its level, -1 leaf
+    int32_t *parent_slot = nullptr; // [node_cap] by data pointer: the parent's list slot (M2M writes it)
+    float4 *poles = nullptr;        // [node_cap][kPoleQ]
+    float4 *locals = nullptr;       // [node_cap][kLocalQ]
+    int32_t *lists[2] = {nullptr, nullptr}; // unchecked-node lists, [branch_cap][list_cap] each
+    int32_t *meta = nullptr;        // device: [0] n_levels, [1] n_nodes, [2] tree_len
+    int64_t node_cap = 0;
+    int64_t level_cap = 0;
+    int64_t branch_cap = 0;         // list slots per level
+    int max_levels = 0;
+    int list_cap = 1024;
+    bool valid = false;
+    // host mirror of the level sizes (known for host trees; upper bounds for GPU trees)
+    int n_levels_host = 0;
+    int level_count_host[16] = {0};
+};
+
+// Scratch of the GPU tree builder (sph_tree.cu).
+struct TreeBuild {
+    RadixSorter sorter;
+    int32_t *nstart = nullptr;  // [max_levels][level_cap]
+    int32_t *ncount = nullptr;  // [max_levels][level_cap]
+    int32_t *nparent = nullptr; // [max_levels][level_cap] parent index in previous level (or -1), octant in high bits
+    int64_t *scan = nullptr;    // [level_cap * 8 + 1] scan scratch
+    int64_t *scan_blocks = nullptr;
+    int32_t *per_particle = nullptr; // [3][n+1] ints at start, nodes at start, first level
+    int32_t *noffset = nullptr; // [max_levels][level_cap] tree offset of each node
+    int32_t *ndp = nullptr;     // [max_levels][level_cap] data pointer
+    float *bbox = nullptr;      // device [6] lo.xyz, hi.xyz as ordered ints
+    int64_t scan_cap = 0;
+};
+
+}  // namespace sph
+
+struct sph_ctx {
+    int n = 0;
+    int device = 0;
+    sph_params params{};
+    std::string forsterite_path, fe_path;
+
+    float4 *pos4 = nullptr, *vel4 = nullptr, *acc4 = nullptr;
+    float *rho = nullptr, *u = nullptr, *P = nullptr, *h = nullptr, *f = nullptr, *c = nullptr;
+    float *du = nullptr, *B = nullptr, *dhdt = nullptr, *gnorm = nullptr;
+    int32_t *mat = nullptr, *nat = nullptr;
+    uint8_t *active = nullptr;
+    int32_t *globals = nullptr;
+    uint32_t *health = nullptr;
+
+    sph::RadixSorter cell_sort;
+    uint2 *cell_range = nullptr;
+    bool cells_have_prev = false;  // cell_range holds the entries of cell_sort.keys[1]
+    int cell_final = 1;            // buffer index of the sorted cell keys
+
+    float4 *sp4 = nullptr, *sv4 = nullptr, *sA = nullptr, *sB = nullptr, *sC = nullptr;
+
+    float2 *eos_forsterite = nullptr, *eos_fe = nullptr;
+    sph::EosTables eos{};
+
+    sph::Tree tree;
+    sph::TreeBuild tb;
+
+    void *stage = nullptr;  // device staging for uploads/downloads
+    size_t stage_bytes = 0;
+    int32_t *snapshot = nullptr;
+
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    cudaStream_t own_stream = nullptr;
+};
+
+namespace sph {
+
+// sph_sort.cu
+sph_status sort_alloc(RadixSorter &s, int n);
+void sort_free(RadixSorter &s);
+// Sort keys[0]/vals[0] (n pairs, `bits` significant key bits) whose digit
+// histograms the producer already accumulated into s.hist.  Returns the buffer
+// index (0/1) that holds the result.
+int radix_sort_pairs(RadixSorter &s, int n, int bits, cudaStream_t st, uint32_t *health);
+sph_status launch_sort(sph_ctx *ctx, cudaStream_t st);
+void launch_init_cells(sph_ctx *ctx, cudaStream_t st);
+// 64-bit exclusive scan of `count` values (count read on the host side bound
+// `n_max`, actual count from *d_count when non-null) into out; *total at out[count].
+void scan_exclusive_i64(const int64_t *in, int64_t *out, int64_t *block_scratch, int n_max, const int32_t *d_count,
+                        cudaStream_t st);
+
+// sph_hydro.cu
+sph_status launch_density(sph_ctx *ctx, cudaStream_t st);
+sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st);
+sph_status launch_step(sph_ctx *ctx, cudaStream_t st);
+sph_status launch_snapshot(sph_ctx *ctx, cudaStream_t st);
+
+// sph_gravity.cu
+sph_status launch_gravity(sph_ctx *ctx, cudaStream_t st);
+
+// sph_tree.cu
+sph_status tree_alloc(sph_ctx *ctx);
+void tree_free(sph_ctx *ctx);
+sph_status launch_tree_build(sph_ctx *ctx, cudaStream_t st);
+
+// sph_api.cu
+void set_error(const char *fmt, ...);
+sph_status cuda_status(cudaError_t e, const char *what);
+
+}  // namespace sph

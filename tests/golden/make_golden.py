@@ -1,0 +1,90 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+The reference ships no tests, golden vectors or known-answer data for its hot
+path, so the fixtures come from the reference's own code run here:
+oracle/ref_build.sh compiles its Metal kernels (SPH/Shaders/*.metal, through a
+host shim), its CPU octree (SPH/octree/octree.cpp) and its ANEOS loader
+(SPH/ANEOS/ANEOS.cpp) unchanged into oracle/_ref/libref.so, and this script
+drives them in the dispatch order of SPH/Compute/Compute.cpp on seeded
+synthetic inputs.  Needs the reference tree (default /root/reference); the
+fixtures are committed so the tests run without it.
+
+    python tests/golden/make_golden.py [reference_root]
+"""
+from __future__ import annotations
+
+import importlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle as O  # noqa: E402
+
+pkg_ic = importlib.import_module("real-time-planetary-impacts-mps_b200.ic")
+pkg_eos = importlib.import_module("real-time-planetary-impacts-mps_b200.eos_tables")
+
+PASS_OUTPUTS = {
+    "sort": ("cell_key", "cell_index"),
+    "gravity": ("acc", "grav_norm", "active"),
+    "density": ("h", "rho", "grad_term", "pressure", "sound_speed", "balsara", "dt"),
+    "acceleration": ("acc", "du", "dhdt", "next_active_time", "dt"),
+    "step": ("pos", "vel", "u", "h", "rho", "global_time"),
+}
+
+
+def occupied_cells(st) -> np.ndarray:
+    occ = np.nonzero(st.cell_start != 0xFFFFFFFF)[0].astype(np.uint32)
+    return np.stack([occ, st.cell_start[occ], st.cell_end[occ]], axis=1)
+
+
+def main(ref_root: str = "/root/reference"):
+    if O.build_ref(ref_root) is None:
+        raise SystemExit(f"reference sources not found under {ref_root}")
+    O.build()
+    tabs = pkg_eos.ensure_tables()
+    # 1. ANEOS loader (ANEOS.cpp) at a reduced resolution
+    np.savez_compressed(os.path.join(HERE, "aneos_res128.npz"),
+                        forsterite=O.aneos_load(tabs["forsterite"], 128, kind="ref"),
+                        fe85si15=O.aneos_load(tabs["Fe85Si15"], 128, kind="ref"))
+    ef = O.aneos_load(tabs["forsterite"], 2048, kind="ref")
+    ee = O.aneos_load(tabs["Fe85Si15"], 2048, kind="ref")
+    # 2. hash + sort + cell ranges on the 16384 + 4096 two-body impact
+    ic = pkg_ic.make_impact(16384, 4096, seed=0)
+    st = O.OracleState(ic, ef, ee, kind="ref")
+    st.sort()
+    np.savez_compressed(os.path.join(HERE, "sort_impact_20480.npz"), pos=ic["pos"], cell_key=st.cell_key,
+                        cell_index=st.cell_index, cells=occupied_cells(st))
+    # 3. the reference's CPU octree at leaf capacities 4 and 32
+    trees = {}
+    for leaf in (4, 32):
+        t = O.tree_reference(ic["pos"], leaf, kind="ref")
+        for k in ("tree", "level_offsets", "level_nodes"):
+            trees[f"leaf{leaf}_{k}"] = t[k]
+        trees[f"leaf{leaf}_meta"] = np.array([t["n_levels"], t["n_nodes"]], np.int32)
+    np.savez_compressed(os.path.join(HERE, "octree_impact_20480.npz"), pos=ic["pos"], **trees)
+    # 4. two full steps of every pass on a 2048 + 512 impact, reference tree (leaf 8)
+    ic = pkg_ic.make_impact(2048, 512, seed=3)
+    st = O.OracleState(ic, ef, ee, kind="ref")
+    out = {f"ic_{k}": np.asarray(v) for k, v in ic.items() if isinstance(v, np.ndarray)}
+    for s in range(2):
+        t = O.tree_reference(st.pos, 8, kind="ref")
+        st.set_tree(t)
+        for k in ("tree", "level_offsets", "level_nodes"):
+            out[f"s{s}_tree_{k}"] = t[k]
+        out[f"s{s}_tree_meta"] = np.array([t["n_levels"], t["n_nodes"]], np.int32)
+        for p, fields in PASS_OUTPUTS.items():
+            getattr(st, p)()
+            for f in fields:
+                out[f"s{s}_{p}_{f}"] = getattr(st, f).copy()
+    np.savez_compressed(os.path.join(HERE, "steps_impact_2560.npz"), **out)
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])
