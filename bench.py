@@ -117,9 +117,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_ic(seed: int):
+_T0 = time.perf_counter()
+
+
+def log(msg: str):
+    print(f"[bench {time.perf_counter() - _T0:8.2f}s] {msg}", file=sys.stderr, flush=True)
+
+
+def make_ic(seed: int, scale: float = 1.0):
     ic_mod = importlib.import_module("real-time-planetary-impacts-mps_b200.ic")
-    return ic_mod.make_impact(N_TARGET, N_IMPACTOR, seed=seed)
+    return ic_mod.make_impact(int(N_TARGET * scale), int(N_IMPACTOR * scale), seed=seed)
 
 
 def cpu_reference(ic: dict, steps: int, warmup: int, budget_s: float | None = None) -> dict:
@@ -181,6 +188,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=float, default=1.0, help="particle count relative to 1e6 (diagnostics)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -199,7 +207,8 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-    ic = make_ic(rank)
+    ic = make_ic(rank, args.scale)
+    log(f"ic ready: {ic['n']} particles")
     n = int(ic["n"])
     c = pkg.Compute(ic, max_children_in_leaf=LEAF, max_tree_depth=DEPTH)
     stream = torch.cuda.Stream()
@@ -207,28 +216,26 @@ def main():
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             c.step(stream)
+            stream.synchronize()
+            log("warm-up step done")
     stream.synchronize()
     c.synchronize()
 
-    # capture K steps with an event between passes into one CUDA graph
+    # the timed region replays K full steps captured into one CUDA graph
     K = args.steps
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(PASSES) + 1)] for _ in range(K)]
     calls = (c.updateOctreeBuffer, c.sort, c.gravitationalPass, c.densityPass, c.accelerationPass, c.stepPass)
     graph = None
     try:
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph, stream=stream):
             for k in range(K):
-                ev[k][0].record(stream)
-                for j, f in enumerate(calls):
+                for f in calls:
                     f(stream)
-                    ev[k][j + 1].record(stream)
         mode = "cuda-graph"
-    except Exception as exc:  # eager launches with the same events
+    except Exception as exc:  # eager launches instead
         graph = None
         mode = f"eager ({type(exc).__name__})"
     stream.synchronize()
-    # a capture does not execute; reset nothing -- the state simply continues
     uuid = None
     try:
         uuid = str(torch.cuda.get_device_properties(local).uuid)
@@ -237,6 +244,7 @@ def main():
     except Exception:
         uuid = None
     sampler = ClockSampler(uuid)
+    log(f"timing mode {mode}")
     sampler.start()
     time.sleep(0.3)
     if dist is not None:
@@ -246,14 +254,13 @@ def main():
     t_end = torch.cuda.Event(enable_timing=True)
     t_start.record(stream)
     if graph is not None:
-        graph.replay()
+        with torch.cuda.stream(stream):  # replay() launches on the current stream
+            graph.replay()
     else:
         with torch.cuda.stream(stream):
             for k in range(K):
-                ev[k][0].record(stream)
-                for j, f in enumerate(calls):
+                for f in calls:
                     f(stream)
-                    ev[k][j + 1].record(stream)
     t_end.record(stream)
     torch.cuda.synchronize()
     if dist is not None:
@@ -265,12 +272,26 @@ def main():
         t = torch.tensor([elapsed_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed_ms = float(t.item())
+    value = world * n * K / (elapsed_ms / 1e3)
+    log(f"timed region: {elapsed_ms / K:.3f} ms/step")
+
+    # per-pass split: K more steps, eager, with an event between passes on the
+    # launching stream (events inside a captured graph cannot be timed)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(PASSES) + 1)] for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            ev[k][0].record(stream)
+            for j, f in enumerate(calls):
+                f(stream)
+                ev[k][j + 1].record(stream)
+    torch.cuda.synchronize()
+    c.synchronize()
     per_pass = {p: 0.0 for p in PASSES}
     for k in range(K):
         for j, p in enumerate(PASSES):
             per_pass[p] += ev[k][j].elapsed_time(ev[k][j + 1])
     per_pass = {p: v / K for p, v in per_pass.items()}
-    value = world * n * K / (elapsed_ms / 1e3)
+    log("per-pass ms: " + ", ".join(f"{p} {v:.3f}" for p, v in per_pass.items()))
 
     # end to end through the public API: host state in, step, host state out
     import ctypes  # noqa: F401
@@ -288,6 +309,7 @@ def main():
             host[f][...] = c.download(f)
     c.synchronize()
     e2e_s = time.perf_counter() - t0
+    log(f"e2e: {e2e_s / args.e2e_steps * 1e3:.2f} ms/step")
     e2e_times = torch.tensor([e2e_s], device="cuda")
     if dist is not None:
         dist.all_reduce(e2e_times, op=dist.ReduceOp.MAX)
@@ -316,7 +338,9 @@ def main():
             "clocks": clocks,
         }
         if not args.no_cpu_baseline and world == 1:
+            log("cpu baseline ...")
             cb = cpu_reference(ic, steps=1, warmup=1, budget_s=30.0)
+            log(f"cpu baseline: {cb['value']:.3e} particle-steps/s on {cb['cores']} cores")
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)
     c.close()

@@ -130,6 +130,13 @@ sph_status sph_set_tree(sph_ctx *ctx, const int32_t *tree, int32_t tree_len, con
 sph_status sph_get_tree(sph_ctx *ctx, int32_t *tree, int64_t tree_room, int32_t *tree_len, int32_t *level_offsets,
                         int32_t *level_nodes, int64_t level_nodes_room, int32_t *n_levels, int32_t *n_nodes);
 
+/* Read back the FMM node records of the last gravity pass (synchronous), by
+ * data pointer: poles 24 floats per node (com.xyz, size | M, XX, XY, XZ | YY,
+ * YZ, ZZ, power2 | min.xyz, minGrav | max.xyz, active | X, Y, Z, 0), locals 16
+ * floats per node (pos.xyz, e0 | e1..e4 | e5..e8 | e9, 0, 0, 0).  Either
+ * pointer may be NULL; n_nodes is the node count of the current tree. */
+sph_status sph_get_tree_nodes(sph_ctx *ctx, float *poles, float *locals, int32_t n_nodes);
+
 /* The passes of Headless::step (Headless.cpp:43-51), in order. */
 sph_status sph_sort(sph_ctx *ctx, void *stream);         /* Compute::sort (Compute.cpp:265-326) */
 sph_status sph_gravity(sph_ctx *ctx, void *stream);      /* Compute::gravitationalPass (:328-377) */

@@ -695,6 +695,8 @@ void ora_sort(ora_state *st) {
     }
 }
 
+static std::vector<float> g_last_poles, g_last_locals;
+
 void ora_gravity(ora_state *st) {
     set_threads();
     if (st->n_levels <= 0 || st->tree_len <= 0) return;
@@ -702,6 +704,31 @@ void ora_gravity(ora_state *st) {
     g.st = st;
     g.cap = st->max_unchecked > 0 ? st->max_unchecked : 1024;
     g.run();
+    // keep the node records, in the CUDA library's layout, for diagnostics
+    const size_t nn = g.poles.size();
+    g_last_poles.assign(nn * 24, 0.f);
+    g_last_locals.assign(nn * 16, 0.f);
+    for (size_t i = 0; i < nn; ++i) {
+        const Pole &p = g.poles[i];
+        float *q = &g_last_poles[i * 24];
+        const float v[24] = {p.pos.x, p.pos.y, p.pos.z, p.size, p.e[M], p.e[XX], p.e[XY], p.e[XZ],
+                             p.e[YY], p.e[YZ], p.e[ZZ], p.power[2], p.mn.x, p.mn.y, p.mn.z, p.min_grav,
+                             p.mx.x, p.mx.y, p.mx.z, p.active ? 1.f : 0.f, p.e[X], p.e[Y], p.e[Z], 0.f};
+        std::memcpy(q, v, sizeof(v));
+        const Loc &l = g.locals[i];
+        float *r = &g_last_locals[i * 16];
+        const float w[16] = {l.pos.x, l.pos.y, l.pos.z, l.e[0], l.e[1], l.e[2], l.e[3], l.e[4],
+                             l.e[5], l.e[6], l.e[7], l.e[8], l.e[9], 0.f, 0.f, 0.f};
+        std::memcpy(r, w, sizeof(w));
+    }
+}
+
+int ora_last_tree_nodes(float *poles, float *locals, int n_nodes) {
+    const int nn = (int)(g_last_poles.size() / 24);
+    if (n_nodes > nn) return -1;
+    if (poles) std::memcpy(poles, g_last_poles.data(), sizeof(float) * 24 * n_nodes);
+    if (locals) std::memcpy(locals, g_last_locals.data(), sizeof(float) * 16 * n_nodes);
+    return nn;
 }
 
 // density.metal:12-239

@@ -63,6 +63,10 @@ void ora_tree_sizes(const ora_tree *t, int32_t *tree_len, int32_t *n_levels, int
 void ora_tree_export(const ora_tree *t, int32_t *tree, int32_t *level_offsets, int32_t *level_nodes);
 void ora_tree_free(ora_tree *t);
 
+/* Node records of the last ora_gravity call, in the CUDA library's layout
+ * (24 floats per multipole, 16 per local, by data pointer); returns the node count. */
+int ora_last_tree_nodes(float *poles, float *locals, int n_nodes);
+
 /* ANEOS text table -> res*res (pressure, sound speed) grid, ANEOS.cpp:21-175.
  * Returns 0 on success, -1 if the file cannot be opened, -2 on short data. */
 int ora_aneos_load(const char *path, int res, float *out);

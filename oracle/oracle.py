@@ -272,3 +272,15 @@ class OracleState:
         for k in ("material", "active", "next_active_time", "global_time", "dt", "cell_key", "cell_index"):
             out[k] = getattr(self, k).copy()
         return out
+
+
+def last_tree_nodes(n_nodes: int):
+    """(poles [n, 24], locals [n, 16]) of the last oracle gravity pass."""
+    lib = load("oracle")
+    lib.ora_last_tree_nodes.argtypes = [_fp, _fp, C.c_int]
+    lib.ora_last_tree_nodes.restype = C.c_int
+    poles = np.zeros((n_nodes, 24), np.float32)
+    locs = np.zeros((n_nodes, 16), np.float32)
+    if lib.ora_last_tree_nodes(ptr(poles, _fp), ptr(locs, _fp), n_nodes) < 0:
+        raise RuntimeError("no gravity pass with that many nodes")
+    return poles, locs

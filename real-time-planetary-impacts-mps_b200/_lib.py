@@ -108,6 +108,7 @@ def load() -> C.CDLL:
         "sph_num_particles": (C.c_int32, [vp]),
         "sph_update_tree": (st, [vp, vp]),
         "sph_get_tree": (st, [vp, _ip, C.c_int64, _ip, _ip, _ip, C.c_int64, _ip, _ip]),
+        "sph_get_tree_nodes": (st, [vp, _fp, _fp, C.c_int32]),
         "sph_set_tree": (st, [vp, _ip, C.c_int32, _ip, _ip, C.c_int32, C.c_int32]),
         "sph_sort": (st, [vp, vp]),
         "sph_gravity": (st, [vp, vp]),

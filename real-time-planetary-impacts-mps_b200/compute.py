@@ -169,6 +169,14 @@ class Compute:
         return dict(tree=tree[:ln.value], level_offsets=off[:nl.value + 1], level_nodes=nodes[:off[nl.value]],
                     n_levels=nl.value, n_nodes=nn.value)
 
+    def get_tree_nodes(self, n_nodes: int):
+        """(poles [n, 24], locals [n, 16]) of the last gravity pass, by data pointer."""
+        poles = np.zeros((n_nodes, 24), np.float32)
+        locs = np.zeros((n_nodes, 16), np.float32)
+        _lib.check(self._lib.sph_get_tree_nodes(self._h, _ptr(poles, _fp), _ptr(locs, _fp), int(n_nodes)),
+                   "sph_get_tree_nodes")
+        return poles, locs
+
     # ---- buffers (Buffers.hpp:14-59) -------------------------------------
     def download(self, field: str) -> np.ndarray:
         n = self.nParticles

@@ -299,7 +299,7 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
             return SPH_ERR_INVALID_ARG;
         }
     for (int i = 0; i < ic->n; ++i)
-        if (!(ic->h[i] > 0.f) || !(ic->h[i] <= kMaxH) || !(ic->mass[i] > 0.f) || !std::isfinite(ic->u[i]) ||
+        if (!(ic->h[i] > 0.f) || !(ic->h[i] <= kMaxInitialH) || !(ic->mass[i] > 0.f) || !std::isfinite(ic->u[i]) ||
             !std::isfinite(ic->rho[i])) {
             set_error("sph_create: bad smoothing length, mass, density or energy at particle %d", i);
             return SPH_ERR_INVALID_ARG;
@@ -454,12 +454,13 @@ sph_status sph_upload(sph_ctx *ctx, sph_field field, const void *host, size_t co
         case SPH_FIELD_U: return f1(ctx->u, 4);
         case SPH_FIELD_PRESSURE: return f1(ctx->P, 4);
         case SPH_FIELD_H: {
-            // smoothing lengths live in (0, MAX_SMOOTHING_LENGTH]; larger ones
-            // would make the neighbour cell box cover the periodic grid many times
+            // the density pass caps h at MAX_SMOOTHING_LENGTH after its first
+            // sweep; a first sweep with h above kMaxInitialH would scan a cell
+            // box wider than the 256-cell periodic grid
             const float *hv = (const float *)host;
             for (size_t i = 0; i < count; ++i)
-                if (!(hv[i] > 0.f) || !(hv[i] <= kMaxH)) {
-                    set_error("sph_upload: smoothing length %g at %zu outside (0, 1]", (double)hv[i], i);
+                if (!(hv[i] > 0.f) || !(hv[i] <= kMaxInitialH)) {
+                    set_error("sph_upload: smoothing length %g at %zu outside (0, 10]", (double)hv[i], i);
                     return SPH_ERR_INVALID_ARG;
                 }
             return f1(ctx->h, 4);
@@ -730,6 +731,19 @@ sph_status sph_get_tree(sph_ctx *ctx, int32_t *tree, int64_t tree_room, int32_t 
         }
     }
     return cuda_status(e, "sph_get_tree");
+}
+
+sph_status sph_get_tree_nodes(sph_ctx *ctx, float *poles, float *locals, int32_t n_nodes) {
+    if (!ctx || n_nodes < 0 || n_nodes > ctx->tree.node_cap) {
+        set_error("sph_get_tree_nodes: bad arguments");
+        return SPH_ERR_INVALID_ARG;
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && poles)
+        e = cudaMemcpy(poles, ctx->tree.poles, sizeof(float4) * kPoleQ * (size_t)n_nodes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && locals)
+        e = cudaMemcpy(locals, ctx->tree.locals, sizeof(float4) * kLocalQ * (size_t)n_nodes, cudaMemcpyDeviceToHost);
+    return cuda_status(e, "sph_get_tree_nodes");
 }
 
 sph_status sph_update_tree(sph_ctx *ctx, void *stream) {

@@ -34,6 +34,9 @@ constexpr uint32_t kNumCells = 1u << (3 * kCellPower);
 constexpr float kG = 6.67e-5f;                       // gravity/poles/poles.h:16
 constexpr float kPi1 = 1 / 3.14159265358979323846f;  // utils/kernels.h:14
 constexpr int kSnapshotRes = 1024;                   // SNAPSHOT_RESOLUTION
+// Largest accepted initial smoothing length: the first density sweep scans a
+// box of floor(4h / CELL_WIDTH) + 1 <= 223 cells per axis, inside the 256-cell grid.
+constexpr float kMaxInitialH = 10.f;
 
 // Multipole record, 6 float4 per node (gravity/poles/poles.h:46-55):
 //   q0 = (com.x, com.y, com.z, size)   q1 = (M, XX, XY, XZ)

@@ -32,8 +32,8 @@ import numpy as np
 
 MATERIALS = {
     # name: (rho0 kg/m^3, K0 Pa, cv J/kg/K, gamma)
-    "forsterite": (3300.0, 1e10, 1000.0, 1.5),
-    "Fe85Si15": (8000.0, 1e10, 450.0, 1.6),
+    "forsterite": (3300.0, 1e9, 1000.0, 1.5),
+    "Fe85Si15": (8000.0, 1e9, 450.0, 1.6),
 }
 FILENAMES = {"forsterite": "ANEOS_forsterite_S19.txt", "Fe85Si15": "ANEOS_Fe85Si15_S20.txt"}
 
@@ -60,7 +60,7 @@ def table_values(material: str, n_rho: int = 96, n_t: int = 96):
 
 def write_table(path: str, material: str, n_rho: int = 96, n_t: int = 96) -> str:
     rho, temp, u, p, c, s = table_values(material, n_rho, n_t)
-    lines = [f"# synthetic stand-in table for {material} (logarithmic cold curve, K0 = 1e10 Pa, + thermal ideal gas)"]
+    lines = [f"# synthetic stand-in table for {material} (logarithmic cold curve, K0 = 1e9 Pa, + thermal ideal gas)"]
     lines += [f"# header line {i}" for i in range(2, 14)]
     lines.append(f"{n_rho} {n_t}")
     for vals in (rho, temp):

