@@ -5,26 +5,27 @@
 // step         SPH/Shaders/step.metal:12-46            (Compute.cpp:242-263)
 // snapshot     SPH/Shaders/render.metal:49-66          (Compute.cpp:396-448)
 //
-// Neighbour passes run one warp per particle, particles taken in sorted
-// (Morton cell) order.  The warp flattens the particle's cell box -- the
-// reference's x-outer, z-inner walk over cells, sorted index within a cell --
-// into one candidate list: it loads 32 cell ranges at a time, prefix-sums
-// their particle counts, and hands candidate t of the list to lane t mod 32.
-// Every lane therefore tests a real candidate in every round, consecutive
-// lanes read consecutive sorted records (coalesced 16-byte loads), and the
-// particle's own control flow (the smoothing-length iteration) is uniform
-// across the warp.  Each lane keeps partial sums that a butterfly reduction
-// combines; every lane ends with the same bits, so the warp takes the same
-// branches.  The visited set of neighbours and all filters are the
-// reference's; only the summation order differs, a rounding-level effect of
-// the same size as FMA contraction.
+// One thread per particle, in sorted (Morton cell) order, so a warp's threads
+// walk neighbouring cells together.  Neighbour data are read from sorted,
+// 16-byte records (sp4/sv4 gathered before density; sA/sB/sC written by the
+// density epilogue), so a cell's particles are one contiguous run instead of
+// the reference's index-chased float3 gathers.
 //
-// Neighbour records are sorted, 16-byte copies (sp4/sv4 gathered before
-// density, sA/sB/sC written by the density epilogue), so a cell's particles
-// are one contiguous run instead of the reference's index-chased float3s.
+// The reference walks the cell box of radius 2h (x outer, z inner; sorted
+// index within a cell) once per smoothing-length iteration and once more for
+// the gradient terms, and the box holds several times more candidates than
+// neighbours.  Here:
+//  * cells whose box lies farther than the filter radius (with a margin for
+//    the rounding of cell boundaries) are skipped: none of their particles
+//    passes the filter, so the visited set and its order are unchanged;
+//  * the first sweep also records, in visiting order, every candidate within
+//    2.5 h of the initial h; later sweeps walk that list with the same
+//    filters while 4h^2 stays inside its radius, and fall back to the box
+//    otherwise.  The list holds every candidate that a later box walk would
+//    accept, in the same order; the two can differ only for candidates at
+//    exactly the kernel's support radius, where W, dW/dh and grad W are zero.
 // The reference's 128-entry per-thread neighbour cache (density.metal:67-70)
-// becomes a rescan of the same box with the same filters (same visited set),
-// and the capped count it keeps is the warp's count, capped.
+// becomes a walk with that cache's filters (its count is kept, capped).
 #include <cuda_runtime.h>
 
 #include "sph_internal.h"
@@ -34,68 +35,35 @@ namespace sph {
 namespace {
 
 constexpr int kHydroThreads = 128;
-constexpr int kHydroWarps = kHydroThreads / 32;
+// Margin on the distance from a particle to a cell box: positions near 318 Mm
+// carry ~3e-5 Mm of float32 rounding, and a particle's cell comes from
+// floor(x / CELL_WIDTH); 2e-4 Mm keeps every particle of the cell inside.
+constexpr float kCellMargin = 2e-4f;
 
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-__device__ __forceinline__ float warp_max(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax_ref(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
+// Squared distance from (px, py, pz) to the box of cell (x, y, z), each axis
+// gap shortened by the margin.
+__device__ __forceinline__ float cell_gap2(float px, float py, float pz, int x, int y, int z) {
+    const float w = kCellWidth;
+    float gx = fmaxf(fmaxf((float)x * w - px, px - (float)(x + 1) * w) - kCellMargin, 0.f);
+    float gy = fmaxf(fmaxf((float)y * w - py, py - (float)(y + 1) * w) - kCellMargin, 0.f);
+    float gz = fmaxf(fmaxf((float)z * w - pz, pz - (float)(z + 1) * w) - kCellMargin, 0.f);
+    return gx * gx + gy * gy + gz * gz;
 }
 
-// Call body(k) on the lanes, once for every candidate k of the cell box b
-// (all lanes pass the same box).  offs: 32 words of per-warp shared memory.
+// The reference's walk over the cell box of radius 2h, skipping cells farther
+// than sqrt(r2cull): body(k) for every remaining candidate, in visiting order.
 template <class F>
-__device__ __forceinline__ void warp_box_sweep(const CellBox &b, const uint2 *__restrict__ cells, uint32_t *offs,
-                                               F &&body) {
-    const int lane = threadIdx.x & 31;
-    const int nx = b.hi0 - b.lo0 + 1, ny = b.hi1 - b.lo1 + 1, nz = b.hi2 - b.lo2 + 1;
-    const int ncell = nx * ny * nz;
-    for (int c0 = 0; c0 < ncell; c0 += 32) {
-        const int j = c0 + lane;
-        uint32_t start = 0u, cnt = 0u;
-        if (j < ncell) {
-            const int zi = j % nz, t = j / nz;
-            const int yi = t % ny, xi = t / ny;
-            const uint2 r = __ldg(cells + cell_index_of(b.lo0 + xi, b.lo1 + yi, b.lo2 + zi));
-            if (r.x != 0xffffffffu) {
-                start = r.x;
-                cnt = r.y - r.x + 1u;
+__device__ __forceinline__ void walk_cells(float px, float py, float pz, float h, float r2cull,
+                                           const uint2 *__restrict__ cells, F &&body) {
+    const CellBox b = cell_box(px, py, pz, h);
+    for (int x = b.lo0; x <= b.hi0; ++x)
+        for (int y = b.lo1; y <= b.hi1; ++y)
+            for (int z = b.lo2; z <= b.hi2; ++z) {
+                if (cell_gap2(px, py, pz, x, y, z) > r2cull) continue;
+                const uint2 r = __ldg(cells + cell_index_of(x, y, z));
+                if (r.x == 0xffffffffu) continue;
+                for (uint32_t k = r.x; k <= r.y; ++k) body(k);
             }
-        }
-        uint32_t incl = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        const uint32_t excl = incl - cnt;
-        for (uint32_t base = 0u; base < total; base += 32u) {
-            // mark where each cell's run starts inside this window of 32
-            // candidates; the cell straddling the window start takes slot 0
-            uint32_t bit = 0u;
-            if (cnt > 0u && excl >= base && excl < base + 32u) {
-                offs[excl - base] = start - excl;
-                bit = 1u << (excl - base);
-            } else if (cnt > 0u && excl < base && incl > base) {
-                offs[0] = start - excl;
-                bit = 1u;
-            }
-            const uint32_t seg = __reduce_or_sync(0xffffffffu, bit);
-            __syncwarp();
-            const uint32_t t = base + (uint32_t)lane;
-            if (t < total) {
-                const int pos = max(0, 31 - __clz(seg & (0xffffffffu >> (31 - lane))));
-                body(offs[pos] + t);
-            }
-            __syncwarp();
-        }
-    }
 }
 
 __global__ void k_gather(int n, const uint32_t *__restrict__ cidx, const float4 *__restrict__ pos4,
@@ -119,34 +87,33 @@ struct DensityArgs {
     float4 *sA, *sB, *sC;
     int32_t *globals;
     uint32_t *health;
+    uint32_t *nlist;  // [kNeighbourListCap][n]: entry s of sorted particle i at s * n + i
     EosTables eos;
 };
 
 __global__ void __launch_bounds__(kHydroThreads) k_density(DensityArgs a) {
-    __shared__ uint32_t s_offs[kHydroWarps][32];
-    uint32_t *offs = s_offs[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    const int index = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // one particle per warp
-    if (index >= a.n) return;                                          // warp-uniform
-    if (index == 0 && lane == 0) a.globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= a.n) return;
+    if (index == 0) a.globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
     const uint32_t ind = a.cidx[index];
     const float4 me = a.sp4[index];
     const float4 mv = a.sv4[index];
     if (!a.active[ind]) {
         // density.metal:40-55: EOS only
-        if (lane == 0) {
-            float2 pc = eos_lookup(a.eos, a.mat[ind], a.rho[ind], a.u[ind]);
-            a.P[ind] = pc.x;
-            a.c[ind] = pc.y;
-            const float hv = a.h[ind], rho = a.rho[ind], fv = a.f[ind];
-            a.sA[index] = make_float4(me.x, me.y, me.z, hv);
-            a.sB[index] = make_float4(mv.x, mv.y, mv.z, pc.y);
-            a.sC[index] = make_float4(me.w, (fv * pc.x / (rho * rho)), rho, a.B[ind]);
-        }
+        const float2 pc = eos_lookup(a.eos, a.mat[ind], a.rho[ind], a.u[ind]);
+        a.P[ind] = pc.x;
+        a.c[ind] = pc.y;
+        const float hv = a.h[ind], rho = a.rho[ind], fv = a.f[ind];
+        a.sA[index] = make_float4(me.x, me.y, me.z, hv);
+        a.sB[index] = make_float4(mv.x, mv.y, mv.z, pc.y);
+        a.sC[index] = make_float4(me.w, (fv * pc.x / (rho * rho)), rho, a.B[ind]);
         return;
     }
     const float px = me.x, py = me.y, pz = me.z, mi = me.w;
     const float4 *__restrict__ sp4 = a.sp4;
+    const uint2 *__restrict__ cells = a.cells;
+    const size_t n = (size_t)a.n;
+    uint32_t *__restrict__ list = a.nlist + index;
     float hi = a.h[ind];
     int max_h = 0;  // an int in the reference (truncates h < 1 to 0)
     float h2x4 = 4.f * hi * hi;
@@ -156,31 +123,59 @@ __global__ void __launch_bounds__(kHydroThreads) k_density(DensityArgs a) {
     int count = 0;
     // The reference's neighbour cache holds the neighbours of the last full
     // scan: that scan's h (box and filter) and its count capped at
-    // N_NEIGHBOURS_ESTIM.  A "cached" sweep rescans with those filters.
+    // N_NEIGHBOURS_ESTIM.  A "cached" sweep walks again with those filters.
     int nn = 0;
     float hs = hi, hs2x4 = h2x4;
+    // neighbour list of radius 2.5 h0, built by the first sweep
+    const float lr = 2.5f * hi;
+    const float lr2 = lr * lr;
+    int nl = 0;
+    bool list_ok = true;
+    bool first = true;
     while (eps > kDensityEta && count < kMaxNR) {
         const bool cached = hi < (float)max_h && nn < kNeighbourCache;
         if (!cached) {
             hs = hi;
             hs2x4 = h2x4;
+            nn = 0;
         }
         const float r2max = cached ? hs2x4 : h2x4;
         const float rlim = cached ? hi + hi : 3.402823466e+38f;
-        float part = 0.f;
-        uint32_t found = 0u;
-        warp_box_sweep(cell_box(px, py, pz, cached ? hs : hi), a.cells, offs, [&](uint32_t k) {
-            const float4 q = __ldg(sp4 + k);
+        dens = 0.f;
+        auto visit = [&](float4 q) {
             const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
             const float r2 = dx * dx + dy * dy + dz * dz;
             if (r2 > r2max) return;
             const float r = sqrtf(r2);
             if (r > rlim) return;
-            ++found;
-            part += kernel_w(r, h1) * q.w;
-        });
-        dens = warp_sum(part);
-        if (!cached) nn = min((int)__reduce_add_sync(0xffffffffu, found), kNeighbourCache);
+            if (!cached && nn < kNeighbourCache) nn++;
+            dens += kernel_w(r, h1) * q.w;
+        };
+        if (first) {
+            // first sweep (never a cached one): walk the 2.5 h box once,
+            // recording the list while summing the sweep of radius 2h
+            first = false;
+            walk_cells(px, py, pz, 1.25f * hi, lr2, cells, [&](uint32_t k) {
+                const float4 q = __ldg(sp4 + k);
+                const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 <= lr2) {
+                    if (nl < kNeighbourListCap)
+                        list[(size_t)nl * n] = k;
+                    else
+                        list_ok = false;
+                    ++nl;
+                }
+                if (r2 > h2x4) return;
+                const float r = sqrtf(r2);
+                if (nn < kNeighbourCache) nn++;
+                dens += kernel_w(r, h1) * q.w;
+            });
+        } else if (list_ok && r2max <= lr2) {
+            for (int s = 0; s < nl; ++s) visit(__ldg(sp4 + list[(size_t)s * n]));
+        } else {
+            walk_cells(px, py, pz, cached ? hs : hi, r2max, cells, [&](uint32_t k) { visit(__ldg(sp4 + k)); });
+        }
         float nh = fmin_ref(kResolutionEta * powf(mi / dens, 1.f / 3), kMaxH);
         nh = 0.5f * (hi + nh);
         eps = fabsf(nh - hi) / hi;
@@ -199,8 +194,8 @@ __global__ void __launch_bounds__(kHydroThreads) k_density(DensityArgs a) {
     const float rlim = cached ? hi + hi : 3.402823466e+38f;
     const float vix = mv.x, viy = mv.y, viz = mv.z;
     const float4 *__restrict__ sv4 = a.sv4;
-    float pd = 0.f, pdh = 0.f, pdiv = 0.f, pcx = 0.f, pcy = 0.f, pcz = 0.f;
-    warp_box_sweep(cell_box(px, py, pz, cached ? hs : hi), a.cells, offs, [&](uint32_t k) {
+    float dens_h = 0.f, vdiv = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+    auto grad = [&](uint32_t k) {
         const float4 q = __ldg(sp4 + k);
         const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
         const float r2 = dx * dx + dy * dy + dz * dz;
@@ -208,25 +203,25 @@ __global__ void __launch_bounds__(kHydroThreads) k_density(DensityArgs a) {
         const float r = sqrtf(r2);
         if (r > rlim) return;
         const float mj = q.w;
-        if (!cached) pd += kernel_w(r, h1) * mj;
-        pdh += mj * kernel_dwdh(r, h1);
+        if (!cached) dens += kernel_w(r, h1) * mj;
+        dens_h += mj * kernel_dwdh(r, h1);
         if (r > 1e-12f) {
             const float r1 = 1.f / r;
             const float4 vj = __ldg(sv4 + k);
             const float vx = vj.x - vix, vy = vj.y - viy, vz = vj.z - viz;
             const float s = kernel_gradw_scale(r, h1);
             const float gx = s * (dx * r1), gy = s * (dy * r1), gz = s * (dz * r1);
-            pdiv += mj * (vx * gx + vy * gy + vz * gz);
-            pcx += mj * (vy * gz - vz * gy);
-            pcy += mj * (vz * gx - vx * gz);
-            pcz += mj * (vx * gy - vy * gx);
+            vdiv += mj * (vx * gx + vy * gy + vz * gz);
+            cx += mj * (vy * gz - vz * gy);
+            cy += mj * (vz * gx - vx * gz);
+            cz += mj * (vx * gy - vy * gx);
         }
-    });
-    if (!cached) dens += warp_sum(pd);
-    const float dens_h = warp_sum(pdh);
-    float vdiv = warp_sum(pdiv);
-    const float cx = warp_sum(pcx), cy = warp_sum(pcy), cz = warp_sum(pcz);
-    if (lane != 0) return;
+    };
+    if (list_ok && r2max <= lr2) {
+        for (int s = 0; s < nl; ++s) grad(list[(size_t)s * n]);
+    } else {
+        walk_cells(px, py, pz, cached ? hs : hi, r2max, cells, grad);
+    }
     vdiv = fabsf(vdiv) / dens;
     const float acurl = sqrtf(cx * cx + cy * cy + cz * cz) / dens;
     const float fi = 1.f / (1.f + (hi / (3.f * dens)) * dens_h);
@@ -256,13 +251,8 @@ struct AccelArgs {
     int32_t *globals;
 };
 
-
-__global__ void __launch_bounds__(kHydroThreads) k_acceleration(AccelArgs a) {
-    __shared__ uint32_t s_offs[kHydroWarps][32];
-    __shared__ int s_min[kHydroWarps];
-    uint32_t *offs = s_offs[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    const int index = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // one particle per warp
+__global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
     int idt = 0x7fffffff;
     if (index < a.n) {
         const uint32_t ind = a.cidx[index];
@@ -273,20 +263,18 @@ __global__ void __launch_bounds__(kHydroThreads) k_acceleration(AccelArgs a) {
             const float facti = Cv.y, rhoi = Cv.z, Bi = Cv.w;
             const float hi1 = 1.f / hi;
             const float hi2x4 = hi * hi * 4.f;
-            const float4 *__restrict__ sA = a.sA;
-            const float4 *__restrict__ sB = a.sB;
-            const float4 *__restrict__ sC = a.sC;
             float dvx = 0.f, dvy = 0.f, dvz = 0.f, du = 0.f, dh = 0.f;
             float vsig_i = 1e-12f;
-            warp_box_sweep(cell_box(xi, yi, zi, fmin_ref(hi, kMaxH)), a.cells, offs, [&](uint32_t k) {
+            const float4 *sA = a.sA, *sB = a.sB, *sC = a.sC;
+            walk_cells(xi, yi, zi, fmin_ref(hi, kMaxH), 3.402823466e+38f, a.cells, [&](uint32_t k) {
                 const float4 Aj = __ldg(sA + k);
                 const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
                 const float r2 = dx * dx + dy * dy + dz * dz;
                 const float hj = Aj.w;
                 const float hj2x4 = hj * hj * 4.f;
-                if ((r2 > hi2x4 && r2 > hj2x4) || r2 < 1e-12f) return;  // accelerations.metal:80
-                const float4 Bj = __ldg(sB + k);
+                if ((r2 > hi2x4 && r2 > hj2x4) || r2 < 1e-12f) return;
                 const float4 Cj = __ldg(sC + k);
+                const float4 Bj = __ldg(sB + k);
                 const float r = sqrtf(r2);
                 const float r1 = 1.f / r;
                 const float mj = Cj.x, factj = Cj.y, rhoj = Cj.z, Balj = Cj.w;
@@ -310,40 +298,34 @@ __global__ void __launch_bounds__(kHydroThreads) k_acceleration(AccelArgs a) {
                 du += mj * (facti * (vx * gix + vy * giy + vz * giz) + 0.5f * nu * (vx * gx + vy * gy + vz * gz));
                 dh += (mj / rhoj) * (vx * gix + vy * giy + vz * giz);
             });
-            dvx = warp_sum(dvx);
-            dvy = warp_sum(dvy);
-            dvz = warp_sum(dvz);
-            du = warp_sum(du);
-            dh = warp_sum(dh);
-            vsig_i = warp_max(vsig_i);
+            float4 acc = a.acc4[ind];
+            acc.x += dvx;
+            acc.y += dvy;
+            acc.z += dvz;
+            a.acc4[ind] = acc;
+            a.du[ind] = du;
+            a.dhdt[ind] = dh;
             // accelerations.metal:129-140
             const float goal = 2.0f * kCFL * kGamma * hi / vsig_i;
-            int rr = 0;
+            int r = 0;
             float cand = kDT0;
-            while (cand > goal && rr < kRMax) {
+            while (cand > goal && r < kRMax) {
                 cand *= 0.5f;
-                rr++;
+                r++;
             }
             idt = (int)ceilf(1 / kDtMin1 * cand);
-            if (lane == 0) {
-                float4 acc = a.acc4[ind];
-                acc.x += dvx;
-                acc.y += dvy;
-                acc.z += dvz;
-                a.acc4[ind] = acc;
-                a.du[ind] = du;
-                a.dhdt[ind] = dh;
-                a.nat[ind] = a.globals[0] + idt;
-            }
+            a.nat[ind] = a.globals[0] + idt;
         }
     }
-    // block-wide minimum of the integer timestep, one atomic per block
-    if (lane == 0) s_min[threadIdx.x >> 5] = idt;
+    // block-wide minimum, then one atomic per block
+    for (int o = 16; o > 0; o >>= 1) idt = min(idt, __shfl_xor_sync(0xffffffffu, idt, o));
+    __shared__ int wmin[32];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = idt;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int v = s_min[0];
-        for (int w = 1; w < kHydroWarps; ++w) v = min(v, s_min[w]);
-        if (v != 0x7fffffff) atomicMin(&a.globals[1], v);
+    if (threadIdx.x < 32) {
+        int v = (threadIdx.x < (blockDim.x >> 5)) ? wmin[threadIdx.x] : 0x7fffffff;
+        for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0 && v != 0x7fffffff) atomicMin(&a.globals[1], v);
     }
 }
 
@@ -428,8 +410,9 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     a.sC = ctx->sC;
     a.globals = ctx->globals;
     a.health = ctx->health;
+    a.nlist = ctx->nlist;
     a.eos = ctx->eos;
-    k_density<<<(n + kHydroWarps - 1) / kHydroWarps, kHydroThreads, 0, st>>>(a);
+    k_density<<<(n + kHydroThreads - 1) / kHydroThreads, kHydroThreads, 0, st>>>(a);
     return cuda_status(cudaGetLastError(), "density");
 }
 
@@ -449,7 +432,7 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     a.nat = ctx->nat;
     a.active = ctx->active;
     a.globals = ctx->globals;
-    k_acceleration<<<(n + kHydroWarps - 1) / kHydroWarps, kHydroThreads, 0, st>>>(a);
+    k_acceleration<<<(n + kHydroThreads - 1) / kHydroThreads, kHydroThreads, 0, st>>>(a);
     return cuda_status(cudaGetLastError(), "acceleration");
 }
 
