@@ -52,18 +52,51 @@ __device__ __forceinline__ float cell_gap2(float px, float py, float pz, int x, 
 
 // The reference's walk over the cell box of radius 2h, skipping cells farther
 // than sqrt(r2cull): body(k) for every remaining candidate, in visiting order.
+//
+// A lane first gathers up to kWalkChunk non-empty cell ranges of its box (in
+// walk order), then runs one flat loop that takes exactly one candidate per
+// iteration and steps to the next range when one runs out.  The lanes of a
+// warp stay in step candidate by candidate, instead of idling while their
+// neighbours finish a longer cell.
+constexpr int kWalkChunk = 32;
+
 template <class F>
 __device__ __forceinline__ void walk_cells(float px, float py, float pz, float h, float r2cull,
                                            const uint2 *__restrict__ cells, F &&body) {
     const CellBox b = cell_box(px, py, pz, h);
-    for (int x = b.lo0; x <= b.hi0; ++x)
-        for (int y = b.lo1; y <= b.hi1; ++y)
-            for (int z = b.lo2; z <= b.hi2; ++z) {
-                if (cell_gap2(px, py, pz, x, y, z) > r2cull) continue;
+    uint2 rg[kWalkChunk];
+    int x = b.lo0, y = b.lo1, z = b.lo2;
+    bool more = true;
+    while (more) {
+        int nc = 0;
+        while (nc < kWalkChunk) {
+            if (cell_gap2(px, py, pz, x, y, z) <= r2cull) {
                 const uint2 r = __ldg(cells + cell_index_of(x, y, z));
-                if (r.x == 0xffffffffu) continue;
-                for (uint32_t k = r.x; k <= r.y; ++k) body(k);
+                if (r.x != 0xffffffffu) rg[nc++] = r;
             }
+            if (++z > b.hi2) {
+                z = b.lo2;
+                if (++y > b.hi1) {
+                    y = b.lo1;
+                    if (++x > b.hi0) {
+                        more = false;
+                        break;
+                    }
+                }
+            }
+        }
+        if (nc == 0) continue;
+        int ci = 0;
+        uint32_t k = rg[0].x, e = rg[0].y;
+        for (;;) {
+            body(k);
+            if (++k > e) {
+                if (++ci >= nc) break;
+                k = rg[ci].x;
+                e = rg[ci].y;
+            }
+        }
+    }
 }
 
 __global__ void k_gather(int n, const uint32_t *__restrict__ cidx, const float4 *__restrict__ pos4,
@@ -249,9 +282,10 @@ struct AccelArgs {
     int32_t *nat;
     const uint8_t *active;
     int32_t *globals;
+    uint32_t *plist;  // accepted pairs, [kNeighbourListCap][n] (the density list's storage)
 };
 
-__global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
+__global__ void __launch_bounds__(kHydroThreads) k_acceleration(AccelArgs a) {
     const int index = blockIdx.x * blockDim.x + threadIdx.x;
     int idt = 0x7fffffff;
     if (index < a.n) {
@@ -263,18 +297,21 @@ __global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
             const float facti = Cv.y, rhoi = Cv.z, Bi = Cv.w;
             const float hi1 = 1.f / hi;
             const float hi2x4 = hi * hi * 4.f;
+            const float4 *__restrict__ sA = a.sA;
+            const float4 *__restrict__ sB = a.sB;
+            const float4 *__restrict__ sC = a.sC;
+            const size_t n = (size_t)a.n;
+            uint32_t *__restrict__ list = a.plist + index;
             float dvx = 0.f, dvy = 0.f, dvz = 0.f, du = 0.f, dh = 0.f;
             float vsig_i = 1e-12f;
-            const float4 *sA = a.sA, *sB = a.sB, *sC = a.sC;
-            walk_cells(xi, yi, zi, fmin_ref(hi, kMaxH), 3.402823466e+38f, a.cells, [&](uint32_t k) {
+            // accelerations.metal:73-120 for one accepted pair
+            auto pair = [&](uint32_t k) {
                 const float4 Aj = __ldg(sA + k);
+                const float4 Bj = __ldg(sB + k);
+                const float4 Cj = __ldg(sC + k);
                 const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
                 const float r2 = dx * dx + dy * dy + dz * dz;
                 const float hj = Aj.w;
-                const float hj2x4 = hj * hj * 4.f;
-                if ((r2 > hi2x4 && r2 > hj2x4) || r2 < 1e-12f) return;
-                const float4 Cj = __ldg(sC + k);
-                const float4 Bj = __ldg(sB + k);
                 const float r = sqrtf(r2);
                 const float r1 = 1.f / r;
                 const float mj = Cj.x, factj = Cj.y, rhoj = Cj.z, Balj = Cj.w;
@@ -297,7 +334,25 @@ __global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
                 dvz -= mj * (facti * giz + factj * gjz + nu * gz);
                 du += mj * (facti * (vx * gix + vy * giy + vz * giz) + 0.5f * nu * (vx * gx + vy * gy + vz * gz));
                 dh += (mj / rhoj) * (vx * gix + vy * giy + vz * giz);
+            };
+            // walk: keep the accepted pairs, in visiting order, then evaluate
+            // them in one uniform loop (a full list is evaluated and emptied)
+            int nl = 0;
+            walk_cells(xi, yi, zi, fmin_ref(hi, kMaxH), 3.402823466e+38f, a.cells, [&](uint32_t k) {
+                const float4 Aj = __ldg(sA + k);
+                const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const float hj = Aj.w;
+                const float hj2x4 = hj * hj * 4.f;
+                if ((r2 > hi2x4 && r2 > hj2x4) || r2 < 1e-12f) return;  // accelerations.metal:80
+                if (nl == kNeighbourListCap) {
+                    for (int s = 0; s < nl; ++s) pair(list[(size_t)s * n]);
+                    nl = 0;
+                }
+                list[(size_t)nl * n] = k;
+                ++nl;
             });
+            for (int s = 0; s < nl; ++s) pair(list[(size_t)s * n]);
             float4 acc = a.acc4[ind];
             acc.x += dvx;
             acc.y += dvy;
@@ -307,11 +362,11 @@ __global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
             a.dhdt[ind] = dh;
             // accelerations.metal:129-140
             const float goal = 2.0f * kCFL * kGamma * hi / vsig_i;
-            int r = 0;
+            int rr = 0;
             float cand = kDT0;
-            while (cand > goal && r < kRMax) {
+            while (cand > goal && rr < kRMax) {
                 cand *= 0.5f;
-                r++;
+                rr++;
             }
             idt = (int)ceilf(1 / kDtMin1 * cand);
             a.nat[ind] = a.globals[0] + idt;
@@ -319,13 +374,13 @@ __global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
     }
     // block-wide minimum, then one atomic per block
     for (int o = 16; o > 0; o >>= 1) idt = min(idt, __shfl_xor_sync(0xffffffffu, idt, o));
-    __shared__ int wmin[32];
+    __shared__ int wmin[kHydroThreads / 32];
     if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = idt;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        int v = (threadIdx.x < (blockDim.x >> 5)) ? wmin[threadIdx.x] : 0x7fffffff;
-        for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (threadIdx.x == 0 && v != 0x7fffffff) atomicMin(&a.globals[1], v);
+    if (threadIdx.x == 0) {
+        int v = wmin[0];
+        for (int w = 1; w < kHydroThreads / 32; ++w) v = min(v, wmin[w]);
+        if (v != 0x7fffffff) atomicMin(&a.globals[1], v);
     }
 }
 
@@ -432,6 +487,7 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     a.nat = ctx->nat;
     a.active = ctx->active;
     a.globals = ctx->globals;
+    a.plist = ctx->nlist;
     k_acceleration<<<(n + kHydroThreads - 1) / kHydroThreads, kHydroThreads, 0, st>>>(a);
     return cuda_status(cudaGetLastError(), "acceleration");
 }
