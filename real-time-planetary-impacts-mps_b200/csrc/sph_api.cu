@@ -267,7 +267,7 @@ sph_status sph_destroy(sph_ctx *ctx) {
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     void *bufs[] = {ctx->pos4, ctx->vel4, ctx->acc4, ctx->rho, ctx->u, ctx->P, ctx->h, ctx->f, ctx->c,
                     ctx->du, ctx->B, ctx->dhdt, ctx->gnorm, ctx->mat, ctx->nat, ctx->active, ctx->globals,
-                    ctx->health, ctx->cell_range, ctx->sp4, ctx->sv4, ctx->sA, ctx->sB, ctx->sC, ctx->nlist,
+                    ctx->health, ctx->cell_range, ctx->sp4, ctx->sv4, ctx->sA, ctx->sB, ctx->sC,
                     ctx->eos_forsterite, ctx->eos_fe, ctx->stage, ctx->snapshot};
     for (void *b : bufs) cudaFree(b);
     sort_free(ctx->cell_sort);
@@ -336,9 +336,7 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     chk(dmalloc(&ctx->globals, 4));
     chk(dmalloc(&ctx->health, 1));
     chk(dmalloc(&ctx->cell_range, (size_t)kNumCells));
-    for (float4 **fp : {&ctx->sp4, &ctx->sv4, &ctx->sA, &ctx->sB, &ctx->sC}) chk(dmalloc(fp, n));
-    chk(dmalloc(&ctx->nlist, (size_t)kNeighbourListCap * n));
-    chk(dmalloc(&ctx->eos_forsterite, (size_t)res * res));
+    for (float4 **fp : {&ctx->sp4, &ctx->sv4, &ctx->sA, &ctx->sB, &ctx->sC}) chk(dmalloc(fp, n));    chk(dmalloc(&ctx->eos_forsterite, (size_t)res * res));
     chk(dmalloc(&ctx->eos_fe, (size_t)res * res));
     ctx->stage_bytes = std::max((size_t)kNumCells * sizeof(uint32_t), sizeof(float) * 3 * (size_t)n);
     chk(cudaMalloc(&ctx->stage, ctx->stage_bytes));

@@ -37,11 +37,6 @@ constexpr int kSnapshotRes = 1024;                   // SNAPSHOT_RESOLUTION
 // Largest accepted initial smoothing length: the first density sweep scans a
 // box of floor(4h / CELL_WIDTH) + 1 <= 223 cells per axis, inside the 256-cell grid.
 constexpr float kMaxInitialH = 10.f;
-// Entries per particle of the density pass's neighbour list (radius 2.5 h);
-// ~60 neighbours lie within 2h, so ~120 within 2.5h.  Longer lists fall back
-// to walking the cell box.
-constexpr int kNeighbourListCap = 192;
-
 // Multipole record, 6 float4 per node (gravity/poles/poles.h:46-55):
 //   q0 = (com.x, com.y, com.z, size)   q1 = (M, XX, XY, XZ)
 //   q2 = (YY, YZ, ZZ, power[2])       q3 = (min.x, min.y, min.z, minGrav)

@@ -5,27 +5,18 @@
 // step         SPH/Shaders/step.metal:12-46            (Compute.cpp:242-263)
 // snapshot     SPH/Shaders/render.metal:49-66          (Compute.cpp:396-448)
 //
-// One thread per particle, in sorted (Morton cell) order, so a warp's threads
+// One thread per particle in sorted (Morton cell) order, so a warp's threads
 // walk neighbouring cells together.  Neighbour data are read from sorted,
-// 16-byte records (sp4/sv4 gathered before density; sA/sB/sC written by the
-// density epilogue), so a cell's particles are one contiguous run instead of
-// the reference's index-chased float3 gathers.
+// 16-byte records (sp4/sv4, then sA/sB/sC written by the density epilogue),
+// so every cell's particles are one contiguous run of float4 loads instead of
+// the reference's index-chased float3 gathers.  The neighbour loops visit
+// cells and particles in the reference's order and accumulate in the same
+// order, so sums agree with it to rounding.
 //
-// The reference walks the cell box of radius 2h (x outer, z inner; sorted
-// index within a cell) once per smoothing-length iteration and once more for
-// the gradient terms, and the box holds several times more candidates than
-// neighbours.  Here:
-//  * cells whose box lies farther than the filter radius (with a margin for
-//    the rounding of cell boundaries) are skipped: none of their particles
-//    passes the filter, so the visited set and its order are unchanged;
-//  * the first sweep also records, in visiting order, every candidate within
-//    2.5 h of the initial h; later sweeps walk that list with the same
-//    filters while 4h^2 stays inside its radius, and fall back to the box
-//    otherwise.  The list holds every candidate that a later box walk would
-//    accept, in the same order; the two can differ only for candidates at
-//    exactly the kernel's support radius, where W, dW/dh and grad W are zero.
 // The reference's 128-entry per-thread neighbour cache (density.metal:67-70)
-// becomes a walk with that cache's filters (its count is kept, capped).
+// is replaced by rescanning the same cell box with the same filters: the
+// visited set and order are identical (see k_density), and no thread carries
+// 1 KiB of local memory.
 #include <cuda_runtime.h>
 
 #include "sph_internal.h"
@@ -34,69 +25,38 @@ namespace sph {
 
 namespace {
 
-constexpr int kHydroThreads = 128;
 // Margin on the distance from a particle to a cell box: positions near 318 Mm
 // carry ~3e-5 Mm of float32 rounding, and a particle's cell comes from
-// floor(x / CELL_WIDTH); 2e-4 Mm keeps every particle of the cell inside.
+// floor(x / CELL_WIDTH); 2e-4 Mm keeps every particle of a cell inside its box.
 constexpr float kCellMargin = 2e-4f;
 
 // Squared distance from (px, py, pz) to the box of cell (x, y, z), each axis
 // gap shortened by the margin.
 __device__ __forceinline__ float cell_gap2(float px, float py, float pz, int x, int y, int z) {
     const float w = kCellWidth;
-    float gx = fmaxf(fmaxf((float)x * w - px, px - (float)(x + 1) * w) - kCellMargin, 0.f);
-    float gy = fmaxf(fmaxf((float)y * w - py, py - (float)(y + 1) * w) - kCellMargin, 0.f);
-    float gz = fmaxf(fmaxf((float)z * w - pz, pz - (float)(z + 1) * w) - kCellMargin, 0.f);
+    const float gx = fmaxf(fmaxf((float)x * w - px, px - (float)(x + 1) * w) - kCellMargin, 0.f);
+    const float gy = fmaxf(fmaxf((float)y * w - py, py - (float)(y + 1) * w) - kCellMargin, 0.f);
+    const float gz = fmaxf(fmaxf((float)z * w - pz, pz - (float)(z + 1) * w) - kCellMargin, 0.f);
     return gx * gx + gy * gy + gz * gz;
 }
 
-// The reference's walk over the cell box of radius 2h, skipping cells farther
-// than sqrt(r2cull): body(k) for every remaining candidate, in visiting order.
-//
-// A lane first gathers up to kWalkChunk non-empty cell ranges of its box (in
-// walk order), then runs one flat loop that takes exactly one candidate per
-// iteration and steps to the next range when one runs out.  The lanes of a
-// warp stay in step candidate by candidate, instead of idling while their
-// neighbours finish a longer cell.
-constexpr int kWalkChunk = 32;
-
+// Visit the neighbours of (px, py, pz) in the cell box of radius 2h, in the
+// reference's order (x outer, z inner; sorted index within a cell).  Cells
+// farther than sqrt(r2cull) are skipped: when r2cull bounds the caller's own
+// distance filter, none of their particles would pass it, so the visited set
+// and its order are unchanged.
 template <class F>
-__device__ __forceinline__ void walk_cells(float px, float py, float pz, float h, float r2cull,
-                                           const uint2 *__restrict__ cells, F &&body) {
-    const CellBox b = cell_box(px, py, pz, h);
-    uint2 rg[kWalkChunk];
-    int x = b.lo0, y = b.lo1, z = b.lo2;
-    bool more = true;
-    while (more) {
-        int nc = 0;
-        while (nc < kWalkChunk) {
-            if (cell_gap2(px, py, pz, x, y, z) <= r2cull) {
-                const uint2 r = __ldg(cells + cell_index_of(x, y, z));
-                if (r.x != 0xffffffffu) rg[nc++] = r;
+__device__ __forceinline__ void for_cells(float px, float py, float pz, float h, float r2cull,
+                                          const uint2 *__restrict__ cells, F &&body) {
+    CellBox b = cell_box(px, py, pz, h);
+    for (int x = b.lo0; x <= b.hi0; ++x)
+        for (int y = b.lo1; y <= b.hi1; ++y)
+            for (int z = b.lo2; z <= b.hi2; ++z) {
+                if (cell_gap2(px, py, pz, x, y, z) > r2cull) continue;
+                uint2 r = __ldg(cells + cell_index_of(x, y, z));
+                if (r.x == 0xffffffffu) continue;
+                for (uint32_t k = r.x; k <= r.y; ++k) body(k);
             }
-            if (++z > b.hi2) {
-                z = b.lo2;
-                if (++y > b.hi1) {
-                    y = b.lo1;
-                    if (++x > b.hi0) {
-                        more = false;
-                        break;
-                    }
-                }
-            }
-        }
-        if (nc == 0) continue;
-        int ci = 0;
-        uint32_t k = rg[0].x, e = rg[0].y;
-        for (;;) {
-            body(k);
-            if (++k > e) {
-                if (++ci >= nc) break;
-                k = rg[ci].x;
-                e = rg[ci].y;
-            }
-        }
-    }
 }
 
 __global__ void k_gather(int n, const uint32_t *__restrict__ cidx, const float4 *__restrict__ pos4,
@@ -120,11 +80,10 @@ struct DensityArgs {
     float4 *sA, *sB, *sC;
     int32_t *globals;
     uint32_t *health;
-    uint32_t *nlist;  // [kNeighbourListCap][n]: entry s of sorted particle i at s * n + i
     EosTables eos;
 };
 
-__global__ void __launch_bounds__(kHydroThreads) k_density(DensityArgs a) {
+__global__ void __launch_bounds__(128) k_density(DensityArgs a) {
     const int index = blockIdx.x * blockDim.x + threadIdx.x;
     if (index >= a.n) return;
     if (index == 0) a.globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
@@ -133,20 +92,16 @@ __global__ void __launch_bounds__(kHydroThreads) k_density(DensityArgs a) {
     const float4 mv = a.sv4[index];
     if (!a.active[ind]) {
         // density.metal:40-55: EOS only
-        const float2 pc = eos_lookup(a.eos, a.mat[ind], a.rho[ind], a.u[ind]);
+        float2 pc = eos_lookup(a.eos, a.mat[ind], a.rho[ind], a.u[ind]);
         a.P[ind] = pc.x;
         a.c[ind] = pc.y;
-        const float hv = a.h[ind], rho = a.rho[ind], fv = a.f[ind];
-        a.sA[index] = make_float4(me.x, me.y, me.z, hv);
+        float hi = a.h[ind], rho = a.rho[ind], fi = a.f[ind];
+        a.sA[index] = make_float4(me.x, me.y, me.z, hi);
         a.sB[index] = make_float4(mv.x, mv.y, mv.z, pc.y);
-        a.sC[index] = make_float4(me.w, (fv * pc.x / (rho * rho)), rho, a.B[ind]);
+        a.sC[index] = make_float4(me.w, (fi * pc.x / (rho * rho)), rho, a.B[ind]);
         return;
     }
     const float px = me.x, py = me.y, pz = me.z, mi = me.w;
-    const float4 *__restrict__ sp4 = a.sp4;
-    const uint2 *__restrict__ cells = a.cells;
-    const size_t n = (size_t)a.n;
-    uint32_t *__restrict__ list = a.nlist + index;
     float hi = a.h[ind];
     int max_h = 0;  // an int in the reference (truncates h < 1 to 0)
     float h2x4 = 4.f * hi * hi;
@@ -154,60 +109,39 @@ __global__ void __launch_bounds__(kHydroThreads) k_density(DensityArgs a) {
     float dens = 0.f;
     float eps = 1.f;
     int count = 0;
-    // The reference's neighbour cache holds the neighbours of the last full
-    // scan: that scan's h (box and filter) and its count capped at
-    // N_NEIGHBOURS_ESTIM.  A "cached" sweep walks again with those filters.
+    // State of the reference's neighbour cache, which holds the neighbours of
+    // the last full scan: that scan's h (box and filter), and its count capped
+    // at N_NEIGHBOURS_ESTIM.  A "cached" sweep is a rescan with those filters.
     int nn = 0;
     float hs = hi, hs2x4 = h2x4;
-    // neighbour list of radius 2.5 h0, built by the first sweep
-    const float lr = 2.5f * hi;
-    const float lr2 = lr * lr;
-    int nl = 0;
-    bool list_ok = true;
-    bool first = true;
+    const uint2 *cells = a.cells;
+    const float4 *sp4 = a.sp4;
     while (eps > kDensityEta && count < kMaxNR) {
-        const bool cached = hi < (float)max_h && nn < kNeighbourCache;
-        if (!cached) {
+        dens = 0.f;
+        if (hi < (float)max_h && nn < kNeighbourCache) {
+            const float h2 = hi + hi;
+            for_cells(px, py, pz, hs, hs2x4, cells, [&](uint32_t k) {
+                float4 q = __ldg(sp4 + k);
+                float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                float r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > hs2x4) return;
+                float r = sqrtf(r2);
+                if (r > h2) return;
+                dens += kernel_w(r, h1) * q.w;
+            });
+        } else {
             hs = hi;
             hs2x4 = h2x4;
             nn = 0;
-        }
-        const float r2max = cached ? hs2x4 : h2x4;
-        const float rlim = cached ? hi + hi : 3.402823466e+38f;
-        dens = 0.f;
-        auto visit = [&](float4 q) {
-            const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 > r2max) return;
-            const float r = sqrtf(r2);
-            if (r > rlim) return;
-            if (!cached && nn < kNeighbourCache) nn++;
-            dens += kernel_w(r, h1) * q.w;
-        };
-        if (first) {
-            // first sweep (never a cached one): walk the 2.5 h box once,
-            // recording the list while summing the sweep of radius 2h
-            first = false;
-            walk_cells(px, py, pz, 1.25f * hi, lr2, cells, [&](uint32_t k) {
-                const float4 q = __ldg(sp4 + k);
-                const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 <= lr2) {
-                    if (nl < kNeighbourListCap)
-                        list[(size_t)nl * n] = k;
-                    else
-                        list_ok = false;
-                    ++nl;
-                }
+            for_cells(px, py, pz, hi, h2x4, cells, [&](uint32_t k) {
+                float4 q = __ldg(sp4 + k);
+                float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                float r2 = dx * dx + dy * dy + dz * dz;
                 if (r2 > h2x4) return;
-                const float r = sqrtf(r2);
+                float r = sqrtf(r2);
                 if (nn < kNeighbourCache) nn++;
                 dens += kernel_w(r, h1) * q.w;
             });
-        } else if (list_ok && r2max <= lr2) {
-            for (int s = 0; s < nl; ++s) visit(__ldg(sp4 + list[(size_t)s * n]));
-        } else {
-            walk_cells(px, py, pz, cached ? hs : hi, r2max, cells, [&](uint32_t k) { visit(__ldg(sp4 + k)); });
         }
         float nh = fmin_ref(kResolutionEta * powf(mi / dens, 1.f / 3), kMaxH);
         nh = 0.5f * (hi + nh);
@@ -220,46 +154,53 @@ __global__ void __launch_bounds__(kHydroThreads) k_density(DensityArgs a) {
             count++;
         }
     }
-    // gradient sweep (density.metal:145-213); with an overflowing cache the
-    // reference adds to the converged density again, and so does this
-    const bool cached = nn < kNeighbourCache;
-    const float r2max = cached ? hs2x4 : h2x4;
-    const float rlim = cached ? hi + hi : 3.402823466e+38f;
-    const float vix = mv.x, viy = mv.y, viz = mv.z;
-    const float4 *__restrict__ sv4 = a.sv4;
+    // gradient sweep (density.metal:145-213)
     float dens_h = 0.f, vdiv = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-    auto grad = [&](uint32_t k) {
-        const float4 q = __ldg(sp4 + k);
-        const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 > r2max) return;
-        const float r = sqrtf(r2);
-        if (r > rlim) return;
-        const float mj = q.w;
-        if (!cached) dens += kernel_w(r, h1) * mj;
+    const float vix = mv.x, viy = mv.y, viz = mv.z;
+    const float4 *sv4 = a.sv4;
+    auto grad = [&](uint32_t k, const float4 &q, float r, float dx, float dy, float dz) {
+        float mj = q.w;
         dens_h += mj * kernel_dwdh(r, h1);
         if (r > 1e-12f) {
-            const float r1 = 1.f / r;
-            const float4 vj = __ldg(sv4 + k);
-            const float vx = vj.x - vix, vy = vj.y - viy, vz = vj.z - viz;
-            const float s = kernel_gradw_scale(r, h1);
-            const float gx = s * (dx * r1), gy = s * (dy * r1), gz = s * (dz * r1);
+            float r1 = 1.f / r;
+            float4 vj = __ldg(sv4 + k);
+            float vx = vj.x - vix, vy = vj.y - viy, vz = vj.z - viz;
+            float s = kernel_gradw_scale(r, h1);
+            float gx = s * (dx * r1), gy = s * (dy * r1), gz = s * (dz * r1);
             vdiv += mj * (vx * gx + vy * gy + vz * gz);
             cx += mj * (vy * gz - vz * gy);
             cy += mj * (vz * gx - vx * gz);
             cz += mj * (vx * gy - vy * gx);
         }
     };
-    if (list_ok && r2max <= lr2) {
-        for (int s = 0; s < nl; ++s) grad(list[(size_t)s * n]);
+    if (nn < kNeighbourCache) {
+        const float h2 = hi + hi;
+        for_cells(px, py, pz, hs, hs2x4, cells, [&](uint32_t k) {
+            float4 q = __ldg(sp4 + k);
+            float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+            float r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > hs2x4) return;
+            float r = sqrtf(r2);
+            if (r > h2) return;
+            grad(k, q, r, dx, dy, dz);
+        });
     } else {
-        walk_cells(px, py, pz, cached ? hs : hi, r2max, cells, grad);
+        // cache overflow: the reference adds to the converged density again
+        for_cells(px, py, pz, hi, h2x4, cells, [&](uint32_t k) {
+            float4 q = __ldg(sp4 + k);
+            float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+            float r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > h2x4) return;
+            float r = sqrtf(r2);
+            dens += kernel_w(r, h1) * q.w;
+            grad(k, q, r, dx, dy, dz);
+        });
     }
     vdiv = fabsf(vdiv) / dens;
-    const float acurl = sqrtf(cx * cx + cy * cy + cz * cz) / dens;
-    const float fi = 1.f / (1.f + (hi / (3.f * dens)) * dens_h);
-    const float2 pc = eos_lookup(a.eos, a.mat[ind], dens, a.u[ind]);
-    const float bal = vdiv / (vdiv + acurl + 1e-4f * (pc.y / hi));
+    float acurl = sqrtf(cx * cx + cy * cy + cz * cz) / dens;
+    float fi = 1.f / (1.f + (hi / (3.f * dens)) * dens_h);
+    float2 pc = eos_lookup(a.eos, a.mat[ind], dens, a.u[ind]);
+    float bal = vdiv / (vdiv + acurl + 1e-4f * (pc.y / hi));
     a.h[ind] = hi;
     a.rho[ind] = dens;
     a.f[ind] = fi;
@@ -282,10 +223,9 @@ struct AccelArgs {
     int32_t *nat;
     const uint8_t *active;
     int32_t *globals;
-    uint32_t *plist;  // accepted pairs, [kNeighbourListCap][n] (the density list's storage)
 };
 
-__global__ void __launch_bounds__(kHydroThreads) k_acceleration(AccelArgs a) {
+__global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
     const int index = blockIdx.x * blockDim.x + threadIdx.x;
     int idt = 0x7fffffff;
     if (index < a.n) {
@@ -297,21 +237,18 @@ __global__ void __launch_bounds__(kHydroThreads) k_acceleration(AccelArgs a) {
             const float facti = Cv.y, rhoi = Cv.z, Bi = Cv.w;
             const float hi1 = 1.f / hi;
             const float hi2x4 = hi * hi * 4.f;
-            const float4 *__restrict__ sA = a.sA;
-            const float4 *__restrict__ sB = a.sB;
-            const float4 *__restrict__ sC = a.sC;
-            const size_t n = (size_t)a.n;
-            uint32_t *__restrict__ list = a.plist + index;
             float dvx = 0.f, dvy = 0.f, dvz = 0.f, du = 0.f, dh = 0.f;
             float vsig_i = 1e-12f;
-            // accelerations.metal:73-120 for one accepted pair
-            auto pair = [&](uint32_t k) {
+            const float4 *sA = a.sA, *sB = a.sB, *sC = a.sC;
+            for_cells(xi, yi, zi, fmin_ref(hi, kMaxH), 3.402823466e+38f, a.cells, [&](uint32_t k) {
                 const float4 Aj = __ldg(sA + k);
-                const float4 Bj = __ldg(sB + k);
-                const float4 Cj = __ldg(sC + k);
                 const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
                 const float r2 = dx * dx + dy * dy + dz * dz;
                 const float hj = Aj.w;
+                const float hj2x4 = hj * hj * 4.f;
+                if ((r2 > hi2x4 && r2 > hj2x4) || r2 < 1e-12f) return;
+                const float4 Cj = __ldg(sC + k);
+                const float4 Bj = __ldg(sB + k);
                 const float r = sqrtf(r2);
                 const float r1 = 1.f / r;
                 const float mj = Cj.x, factj = Cj.y, rhoj = Cj.z, Balj = Cj.w;
@@ -334,25 +271,7 @@ __global__ void __launch_bounds__(kHydroThreads) k_acceleration(AccelArgs a) {
                 dvz -= mj * (facti * giz + factj * gjz + nu * gz);
                 du += mj * (facti * (vx * gix + vy * giy + vz * giz) + 0.5f * nu * (vx * gx + vy * gy + vz * gz));
                 dh += (mj / rhoj) * (vx * gix + vy * giy + vz * giz);
-            };
-            // walk: keep the accepted pairs, in visiting order, then evaluate
-            // them in one uniform loop (a full list is evaluated and emptied)
-            int nl = 0;
-            walk_cells(xi, yi, zi, fmin_ref(hi, kMaxH), 3.402823466e+38f, a.cells, [&](uint32_t k) {
-                const float4 Aj = __ldg(sA + k);
-                const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                const float hj = Aj.w;
-                const float hj2x4 = hj * hj * 4.f;
-                if ((r2 > hi2x4 && r2 > hj2x4) || r2 < 1e-12f) return;  // accelerations.metal:80
-                if (nl == kNeighbourListCap) {
-                    for (int s = 0; s < nl; ++s) pair(list[(size_t)s * n]);
-                    nl = 0;
-                }
-                list[(size_t)nl * n] = k;
-                ++nl;
             });
-            for (int s = 0; s < nl; ++s) pair(list[(size_t)s * n]);
             float4 acc = a.acc4[ind];
             acc.x += dvx;
             acc.y += dvy;
@@ -362,11 +281,11 @@ __global__ void __launch_bounds__(kHydroThreads) k_acceleration(AccelArgs a) {
             a.dhdt[ind] = dh;
             // accelerations.metal:129-140
             const float goal = 2.0f * kCFL * kGamma * hi / vsig_i;
-            int rr = 0;
+            int r = 0;
             float cand = kDT0;
-            while (cand > goal && rr < kRMax) {
+            while (cand > goal && r < kRMax) {
                 cand *= 0.5f;
-                rr++;
+                r++;
             }
             idt = (int)ceilf(1 / kDtMin1 * cand);
             a.nat[ind] = a.globals[0] + idt;
@@ -374,13 +293,13 @@ __global__ void __launch_bounds__(kHydroThreads) k_acceleration(AccelArgs a) {
     }
     // block-wide minimum, then one atomic per block
     for (int o = 16; o > 0; o >>= 1) idt = min(idt, __shfl_xor_sync(0xffffffffu, idt, o));
-    __shared__ int wmin[kHydroThreads / 32];
+    __shared__ int wmin[32];
     if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = idt;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int v = wmin[0];
-        for (int w = 1; w < kHydroThreads / 32; ++w) v = min(v, wmin[w]);
-        if (v != 0x7fffffff) atomicMin(&a.globals[1], v);
+    if (threadIdx.x < 32) {
+        int v = (threadIdx.x < (blockDim.x >> 5)) ? wmin[threadIdx.x] : 0x7fffffff;
+        for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0 && v != 0x7fffffff) atomicMin(&a.globals[1], v);
     }
 }
 
@@ -465,9 +384,8 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     a.sC = ctx->sC;
     a.globals = ctx->globals;
     a.health = ctx->health;
-    a.nlist = ctx->nlist;
     a.eos = ctx->eos;
-    k_density<<<(n + kHydroThreads - 1) / kHydroThreads, kHydroThreads, 0, st>>>(a);
+    k_density<<<(n + 127) / 128, 128, 0, st>>>(a);
     return cuda_status(cudaGetLastError(), "density");
 }
 
@@ -487,8 +405,7 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     a.nat = ctx->nat;
     a.active = ctx->active;
     a.globals = ctx->globals;
-    a.plist = ctx->nlist;
-    k_acceleration<<<(n + kHydroThreads - 1) / kHydroThreads, kHydroThreads, 0, st>>>(a);
+    k_acceleration<<<(n + 127) / 128, 128, 0, st>>>(a);
     return cuda_status(cudaGetLastError(), "acceleration");
 }
 

@@ -100,8 +100,6 @@ struct sph_ctx {
     int cell_final = 1;            // buffer index of the sorted cell keys
 
     float4 *sp4 = nullptr, *sv4 = nullptr, *sA = nullptr, *sB = nullptr, *sC = nullptr;
-    uint32_t *nlist = nullptr;  // density neighbour lists, [kNeighbourListCap][n]
-
     float2 *eos_forsterite = nullptr, *eos_fe = nullptr;
     sph::EosTables eos{};
 
