@@ -144,6 +144,26 @@ sph_status sph_density(sph_ctx *ctx, void *stream);      /* Compute::densityPass
 sph_status sph_acceleration(sph_ctx *ctx, void *stream); /* Compute::accelerationPass (:210-240) */
 sph_status sph_step(sph_ctx *ctx, void *stream);         /* Compute::stepPass (:242-263) */
 
+/* Cell sort for callers that cannot allocate device memory.  No counterpart in
+ * the reference.  Meant for code whose host framework owns every device
+ * allocation (pools, arenas, memory accounting), or that must not call
+ * cudaMalloc/cudaFree on a latency-critical thread because those calls can
+ * synchronise the device.  From positions the caller already holds on the
+ * device (pos_xyz: 3n floats, xyz interleaved) it writes the same sorted
+ * (cell key, particle index) pairs that sph_sort produces (SPH_FIELD_CELL_KEY,
+ * SPH_FIELD_CELL_INDEX) into cell_key and cell_index (n entries each, device
+ * memory).  It allocates nothing: its scratch is one fixed array inside the
+ * library, present on every GPU that loads the library until the process
+ * exits, which bounds n to SPH_SORT_NOALLOC_MAX_N (larger n is rejected with
+ * SPH_ERR_INVALID_ARG).  The first call on each device looks up that array's
+ * device address; make that first call before any stream capture.  Every call
+ * reuses the array, so calls that overlap on the GPU (unordered streams,
+ * several host threads) race; order them on one stream.  Asynchronous on
+ * `stream`; no context is needed. */
+#define SPH_SORT_NOALLOC_MAX_N 262144
+sph_status sph_sort_cells_noalloc(const float *pos_xyz, int32_t n, uint32_t *cell_key, uint32_t *cell_index,
+                                  void *stream);
+
 /* n_steps x (tree, sort, gravity, density, acceleration, step), replayed from
  * a CUDA graph captured on first use (Headless::step without the snapshot). */
 sph_status sph_step_all(sph_ctx *ctx, void *stream, int32_t n_steps);

@@ -116,6 +116,7 @@ def load() -> C.CDLL:
         "sph_acceleration": (st, [vp, vp]),
         "sph_step": (st, [vp, vp]),
         "sph_step_all": (st, [vp, vp, C.c_int32]),
+        "sph_sort_cells_noalloc": (st, [vp, C.c_int32, vp, vp, vp]),
         "sph_draw_snapshot": (st, [vp, vp, _ip]),
         "sph_upload": (st, [vp, C.c_int, vp, C.c_size_t]),
         "sph_download": (st, [vp, C.c_int, vp, C.c_size_t]),

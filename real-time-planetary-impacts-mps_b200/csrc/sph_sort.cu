@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <mutex>
 
 #include "sph_internal.h"
 
@@ -354,3 +355,134 @@ sph_status launch_sort(sph_ctx *ctx, cudaStream_t st) {
 }
 
 }  // namespace sph
+
+// ---------------------------------------------------------------------------
+// Cell sort without allocation.
+//
+// Some callers cannot allocate device memory at all: code that runs inside a
+// host framework which owns every allocation (a pool or arena it hands out,
+// memory-accounting or sandboxing layers), or code that must not call
+// cudaMalloc/cudaFree on a latency-critical thread because those calls may
+// synchronise the device.  For them, sph_sort_cells_noalloc computes the same
+// sorted (cell key, particle index) pairs as sph_sort from positions the
+// caller already holds on the device, using only caller-provided inputs and
+// outputs plus one fixed scratch array compiled into this library.
+//
+// The scratch is a file-scope __device__ array, so every GPU that loads the
+// library carries it (kNoAllocScratchBytes, about 2.2 MiB) until the process
+// exits.  On the host, the array's name is only a stand-in symbol, not a
+// device address; its device address is looked up once per device with
+// cudaGetSymbolAddress, on the first call made while that device is current.
+// Every call shares the array and it keeps the last call's contents, so the
+// parts that must start at zero are cleared on the caller's stream at each
+// call, and calls whose work overlaps on the GPU (different streams without
+// ordering, or several host threads) race on it.
+// ---------------------------------------------------------------------------
+namespace sph {
+namespace {
+
+constexpr int kNoAllocPasses = 3;  // 24-bit cell keys
+constexpr int kNoAllocTiles = (SPH_SORT_NOALLOC_MAX_N + RadixSorter::kTile - 1) / RadixSorter::kTile;
+constexpr size_t kNoAllocKeysOff = 0;
+constexpr size_t kNoAllocValsOff = kNoAllocKeysOff + sizeof(uint32_t) * SPH_SORT_NOALLOC_MAX_N;
+constexpr size_t kNoAllocHistOff = kNoAllocValsOff + sizeof(uint32_t) * SPH_SORT_NOALLOC_MAX_N;
+constexpr size_t kNoAllocStatusOff = kNoAllocHistOff + sizeof(uint32_t) * 256 * kNoAllocPasses;
+constexpr size_t kNoAllocCountOff = kNoAllocStatusOff + sizeof(uint32_t) * 256 * kNoAllocTiles * kNoAllocPasses;
+constexpr size_t kNoAllocHealthOff = kNoAllocCountOff + sizeof(uint32_t) * kNoAllocPasses;
+constexpr size_t kNoAllocScratchBytes = kNoAllocHealthOff + sizeof(uint32_t);
+// bytes that must be zero when a call starts: histograms, look-back words,
+// tile tickets and the health word
+constexpr size_t kNoAllocZeroBytes = kNoAllocScratchBytes - kNoAllocHistOff;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_dev[kNoAllocMaxDevices] = {};
+
+// sort.metal:15-44 from xyz-interleaved positions, plus the digit histograms
+// of the three passes (same keys as k_hash_hist; no cell table to clear).
+__global__ void k_hash_hist_xyz(const float *__restrict__ pos, int n, uint32_t *__restrict__ keys,
+                                uint32_t *__restrict__ vals, uint32_t *__restrict__ hist) {
+    __shared__ uint32_t sh[3][256];
+    for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&sh[0][0])[i] = 0u;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = cell_key(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        keys[i] = k;
+        vals[i] = (uint32_t)i;
+        atomicAdd(&sh[0][k & 255u], 1u);
+        atomicAdd(&sh[1][(k >> 8) & 255u], 1u);
+        atomicAdd(&sh[2][(k >> 16) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) {
+        const uint32_t v = (&sh[0][0])[i];
+        if (v) atomicAdd(hist + i, v);
+    }
+}
+
+// Device address of the scratch array on the current device (set-up on first use).
+sph_status noalloc_scratch(unsigned char **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e, "sph_sort_cells_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error("sph_sort_cells_noalloc: device ordinal %d is not supported", dev);
+        return SPH_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_dev[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e, "sph_sort_cells_noalloc: cudaGetSymbolAddress");
+        g_noalloc_dev[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_noalloc_dev[dev];
+    return SPH_OK;
+}
+
+}  // namespace
+
+}  // namespace sph
+
+extern "C" sph_status sph_sort_cells_noalloc(const float *pos_xyz, int32_t n, uint32_t *cell_key,
+                                            uint32_t *cell_index, void *stream) {
+    using namespace sph;
+    if (n < 0 || n > SPH_SORT_NOALLOC_MAX_N) {
+        set_error("sph_sort_cells_noalloc: n = %d is outside 0..%d (the size of the library's fixed scratch)", n,
+                  SPH_SORT_NOALLOC_MAX_N);
+        return SPH_ERR_INVALID_ARG;
+    }
+    if (n == 0) return SPH_OK;
+    if (!pos_xyz || !cell_key || !cell_index) {
+        set_error("sph_sort_cells_noalloc: null device pointer");
+        return SPH_ERR_INVALID_ARG;
+    }
+    unsigned char *s = nullptr;
+    sph_status st = noalloc_scratch(&s);
+    if (st != SPH_OK) return st;
+    cudaStream_t cs = (cudaStream_t)stream;
+    uint32_t *tk = reinterpret_cast<uint32_t *>(s + kNoAllocKeysOff);
+    uint32_t *tv = reinterpret_cast<uint32_t *>(s + kNoAllocValsOff);
+    uint32_t *hist = reinterpret_cast<uint32_t *>(s + kNoAllocHistOff);
+    uint32_t *status = reinterpret_cast<uint32_t *>(s + kNoAllocStatusOff);
+    uint32_t *counters = reinterpret_cast<uint32_t *>(s + kNoAllocCountOff);
+    uint32_t *health = reinterpret_cast<uint32_t *>(s + kNoAllocHealthOff);
+    cudaError_t e = cudaMemsetAsync(s + kNoAllocHistOff, 0, kNoAllocZeroBytes, cs);
+    if (e != cudaSuccess) return cuda_status(e, "sph_sort_cells_noalloc: clear scratch");
+    int blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_hash_hist_xyz<<<blocks, 256, 0, cs>>>(pos_xyz, n, tk, tv, hist);
+    // three stable 8-bit passes: scratch -> out -> scratch -> out
+    const int tiles = (n + RadixSorter::kTile - 1) / RadixSorter::kTile;
+    uint32_t *kin[kNoAllocPasses] = {tk, cell_key, tk};
+    uint32_t *vin[kNoAllocPasses] = {tv, cell_index, tv};
+    uint32_t *kout[kNoAllocPasses] = {cell_key, tk, cell_key};
+    uint32_t *vout[kNoAllocPasses] = {cell_index, tv, cell_index};
+    for (int p = 0; p < kNoAllocPasses; ++p)
+        k_onesweep<<<tiles, RadixSorter::kThreads, 0, cs>>>(kin[p], vin[p], kout[p], vout[p], n, 8 * p, hist + 256 * p,
+                                                            status + (size_t)256 * kNoAllocTiles * p, counters + p,
+                                                            health);
+    return cuda_status(cudaGetLastError(), "sph_sort_cells_noalloc");
+}
