@@ -102,7 +102,8 @@ typedef enum {
     SPH_FIELD_CELL_INDEX = 20,  /* U   _cellArrayi[].y after sort (n) */
     SPH_FIELD_CELL_START = 21,  /* U   _cellStart (2^24), UINT_MAX when empty; download only */
     SPH_FIELD_CELL_END = 22,    /* U   _cellEnd (2^24), 0 when empty; download only */
-    SPH_FIELD_COUNT = 23
+    SPH_FIELD_POTENTIAL = 23,   /* F   gravitational potential G phi (SPH_GRAVITY_THETA only; no reference buffer) */
+    SPH_FIELD_COUNT = 24
 } sph_field;
 
 /* Defaults equal to SPH/Parameters.h (table paths are the reference's names). */
@@ -143,6 +144,30 @@ sph_status sph_gravity(sph_ctx *ctx, void *stream);      /* Compute::gravitation
 sph_status sph_density(sph_ctx *ctx, void *stream);      /* Compute::densityPass (:179-208) */
 sph_status sph_acceleration(sph_ctx *ctx, void *stream); /* Compute::accelerationPass (:210-240) */
 sph_status sph_step(sph_ctx *ctx, void *stream);         /* Compute::stepPass (:242-263) */
+
+/* Numerical forms beside the reference's own.  None has a counterpart in the
+ * reference; the default form (all zero) reproduces the reference's logic,
+ * quirks included, and is what the parity tests check against it. */
+#define SPH_GRAVITY_REFERENCE 0 /* adaptive acceptance, forced leaf M2L, truncated softening (Compute.cpp:328-377) */
+#define SPH_GRAVITY_THETA     1 /* opening angle theta, quadrupole M2L/M2P, exact softened P2P, Kahan sums */
+typedef struct {
+    int32_t gravity; /* SPH_GRAVITY_* */
+    float theta;     /* opening angle of SPH_GRAVITY_THETA: accept when r_A + r_B < theta |com_A - com_B| */
+    int32_t h_seed;  /* reserved, 0 */
+    int32_t precision; /* reserved, 0 */
+} sph_form;
+void sph_form_default(sph_form *f); /* reference form, theta 0.5 */
+/* Select the form for the following passes (drops a captured step graph). */
+sph_status sph_set_form(sph_ctx *ctx, const sph_form *f);
+sph_status sph_get_form(const sph_ctx *ctx, sph_form *f);
+
+/* FP64 direct-sum gravity at n_targets particles (host array of particle
+ * indices), from the current positions and masses of all particles, with the
+ * cubic-spline softened kernel and its exact coefficients: out receives
+ * (ax, ay, az, phi) per target, G included.  The accuracy reference for the
+ * gravity forms; no counterpart in the reference.  Synchronous. */
+sph_status sph_gravity_direct_f64(sph_ctx *ctx, const int32_t *targets, int32_t n_targets, double *out,
+                                  void *stream);
 
 /* Cell sort for callers that cannot allocate device memory.  No counterpart in
  * the reference.  Meant for code whose host framework owns every device

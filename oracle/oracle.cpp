@@ -1219,4 +1219,51 @@ int ora_aneos_load(const char *path, int res, float *out) {
     return 0;
 }
 
+// FP64 direct-sum gravity (no reference counterpart): the accuracy reference
+// of the gravity forms.  Cubic-spline softened kernel with its exact
+// coefficients (Price & Monaghan 2007 form; the reference's kernels.h:87-102
+// truncates them), softening length GRAVITY_SMOOTHING_LENGTH = 0.04
+// (Parameters.h), G = 6.67e-5 in code units (gravity/poles/poles.h:16).
+void ora_gravity_direct_f64(int n, const float *pos3, const float *mass, const int32_t *targets, int nt,
+                            double *out) {
+    set_threads();
+    const double G = (double)6.67e-5f, h = (double)0.04f, h1 = 1.0 / h;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int t = 0; t < nt; ++t) {
+        const int i = targets[t];
+        const double xi = pos3[3 * i], yi = pos3[3 * i + 1], zi = pos3[3 * i + 2];
+        double ax = 0.0, ay = 0.0, az = 0.0, ph = 0.0;
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            const double rx = xi - pos3[3 * j], ry = yi - pos3[3 * j + 1], rz = zi - pos3[3 * j + 2];
+            const double r2 = rx * rx + ry * ry + rz * rz;
+            if (r2 == 0.0) continue;
+            const double r = std::sqrt(r2), q = r * h1;
+            double fr, pot;
+            if (q >= 2.0) {
+                fr = 1.0 / r2;
+                pot = -1.0 / r;
+            } else if (q > 1.0) {
+                const double q2 = q * q;
+                fr = h1 * h1 * ((8.0 / 3.0) * q - 3.0 * q2 + 1.2 * q2 * q - q2 * q2 / 6.0 - 1.0 / (15.0 * q2));
+                pot = h1 * ((4.0 / 3.0) * q2 - q2 * q + 0.3 * q2 * q2 - q2 * q2 * q / 30.0 - 1.6 + 1.0 / (15.0 * q));
+            } else {
+                const double q2 = q * q;
+                fr = h1 * h1 * ((4.0 / 3.0) * q - 1.2 * q2 * q + 0.5 * q2 * q2);
+                pot = h1 * ((2.0 / 3.0) * q2 - 0.3 * q2 * q2 + 0.1 * q2 * q2 * q - 1.4);
+            }
+            const double m = mass[j];
+            const double s = -m * fr / r;
+            ax += s * rx;
+            ay += s * ry;
+            az += s * rz;
+            ph += m * pot;
+        }
+        out[4 * (size_t)t + 0] = G * ax;
+        out[4 * (size_t)t + 1] = G * ay;
+        out[4 * (size_t)t + 2] = G * az;
+        out[4 * (size_t)t + 3] = G * ph;
+    }
+}
+
 }  // extern "C"

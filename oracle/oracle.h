@@ -74,6 +74,11 @@ int ora_aneos_load(const char *path, int res, float *out);
 /* Morton cell key of one position (sort.metal:15-44), exposed for tests. */
 uint32_t ora_cell_key(float x, float y, float z);
 
+/* FP64 direct-sum gravity at nt target particles: out[4 t] = (ax, ay, az, phi),
+ * G included, exact cubic-spline softening (no reference counterpart). */
+void ora_gravity_direct_f64(int n, const float *pos3, const float *mass, const int32_t *targets, int nt,
+                            double *out);
+
 /* Threads used by the OpenMP loops (0 = library default). */
 void ora_set_threads(int n);
 int ora_get_threads(void);

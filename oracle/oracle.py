@@ -95,6 +95,8 @@ def load(kind: str = "oracle") -> C.CDLL:
         lib.ora_aneos_load.restype = C.c_int
         lib.ora_cell_key.argtypes = [C.c_float, C.c_float, C.c_float]
         lib.ora_cell_key.restype = C.c_uint32
+        lib.ora_gravity_direct_f64.argtypes = [C.c_int, _fp, _fp, _ip, C.c_int, C.POINTER(C.c_double)]
+        lib.ora_gravity_direct_f64.restype = None
         lib.ora_set_threads.argtypes = [C.c_int]
         lib.ora_get_threads.restype = C.c_int
     elif kind == "ref":
@@ -114,6 +116,18 @@ def load(kind: str = "oracle") -> C.CDLL:
         raise ValueError(kind)
     _LIBS[kind] = lib
     return lib
+
+
+def gravity_direct_f64(pos: np.ndarray, mass: np.ndarray, targets) -> np.ndarray:
+    """FP64 direct-sum (ax, ay, az, phi) at the target particles, G included."""
+    lib = load("oracle")
+    p = np.ascontiguousarray(np.asarray(pos, np.float32).reshape(-1))
+    m = np.ascontiguousarray(np.asarray(mass, np.float32).reshape(-1))
+    t = np.ascontiguousarray(np.asarray(targets, np.int32).reshape(-1))
+    out = np.zeros((t.size, 4), np.float64)
+    lib.ora_gravity_direct_f64(int(m.size), p.ctypes.data_as(_fp), m.ctypes.data_as(_fp), t.ctypes.data_as(_ip),
+                               int(t.size), out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
 
 
 def ptr(a: np.ndarray, t):

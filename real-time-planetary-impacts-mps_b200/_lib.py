@@ -13,7 +13,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "libsph_b200.so")
-SOURCES = ["sph_api.cu", "sph_sort.cu", "sph_hydro.cu", "sph_gravity.cu", "sph_tree.cu"]
+SOURCES = ["sph_api.cu", "sph_sort.cu", "sph_hydro.cu", "sph_gravity.cu", "sph_gravity_theta.cu", "sph_tree.cu"]
 HEADERS = ["sph_common.cuh", "sph_internal.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared"]
@@ -25,11 +25,14 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "i/o err
 SPH_TREE_GPU = 0
 SPH_TREE_HOST = 1
 
+SPH_GRAVITY_REFERENCE = 0
+SPH_GRAVITY_THETA = 1
+
 FIELDS = {
     "pos": 0, "vel": 1, "acc": 2, "rho": 3, "u": 4, "mass": 5, "pressure": 6, "h": 7,
     "grad_term": 8, "sound_speed": 9, "du": 10, "balsara": 11, "dhdt": 12, "grav_norm": 13,
     "material": 14, "active": 15, "next_active_time": 16, "global_time": 17, "dt": 18,
-    "cell_key": 19, "cell_index": 20, "cell_start": 21, "cell_end": 22,
+    "cell_key": 19, "cell_index": 20, "cell_start": 21, "cell_end": 22, "potential": 23,
 }
 VECTOR_FIELDS = ("pos", "vel", "acc")
 
@@ -59,6 +62,10 @@ class SphIC(C.Structure):
         ("pos", _fp), ("vel", _fp), ("rho", _fp), ("u", _fp), ("mass", _fp), ("pressure", _fp), ("h", _fp),
         ("material", _ip),
     ]
+
+
+class SphForm(C.Structure):
+    _fields_ = [("gravity", C.c_int32), ("theta", C.c_float), ("h_seed", C.c_int32), ("precision", C.c_int32)]
 
 
 class SphError(RuntimeError):
@@ -117,6 +124,10 @@ def load() -> C.CDLL:
         "sph_step": (st, [vp, vp]),
         "sph_step_all": (st, [vp, vp, C.c_int32]),
         "sph_sort_cells_noalloc": (st, [vp, C.c_int32, vp, vp, vp]),
+        "sph_form_default": (None, [C.POINTER(SphForm)]),
+        "sph_set_form": (st, [vp, C.POINTER(SphForm)]),
+        "sph_get_form": (st, [vp, C.POINTER(SphForm)]),
+        "sph_gravity_direct_f64": (st, [vp, _ip, C.c_int32, C.POINTER(C.c_double), vp]),
         "sph_draw_snapshot": (st, [vp, vp, _ip]),
         "sph_upload": (st, [vp, C.c_int, vp, C.c_size_t]),
         "sph_download": (st, [vp, C.c_int, vp, C.c_size_t]),

@@ -169,6 +169,30 @@ class Compute:
         return dict(tree=tree[:ln.value], level_offsets=off[:nl.value + 1], level_nodes=nodes[:off[nl.value]],
                     n_levels=nl.value, n_nodes=nn.value)
 
+    # ---- numerical forms (no reference counterpart) --------------------
+    def set_form(self, gravity: str = "reference", theta: float = 0.5):
+        """Select the gravity form: "reference" (the reference's logic) or
+        "theta" (opening-angle FMM with exact near field)."""
+        f = _lib.SphForm()
+        self._lib.sph_form_default(C.byref(f))
+        f.gravity = _lib.SPH_GRAVITY_THETA if gravity == "theta" else _lib.SPH_GRAVITY_REFERENCE
+        f.theta = float(theta)
+        _lib.check(self._lib.sph_set_form(self._h, C.byref(f)), "sph_set_form")
+
+    def get_form(self) -> dict:
+        f = _lib.SphForm()
+        _lib.check(self._lib.sph_get_form(self._h, C.byref(f)), "sph_get_form")
+        return dict(gravity="theta" if f.gravity == _lib.SPH_GRAVITY_THETA else "reference", theta=f.theta)
+
+    def gravity_direct_f64(self, targets, stream=None) -> np.ndarray:
+        """FP64 direct-sum (ax, ay, az, phi) at the given particles, G included."""
+        t = np.ascontiguousarray(np.asarray(targets, np.int32).reshape(-1))
+        out = np.zeros((t.size, 4), np.float64)
+        _lib.check(self._lib.sph_gravity_direct_f64(self._h, _ptr(t, _ip), int(t.size),
+                                                    out.ctypes.data_as(C.POINTER(C.c_double)), _stream(stream)),
+                   "sph_gravity_direct_f64")
+        return out
+
     def get_tree_nodes(self, n_nodes: int):
         """(poles [n, 24], locals [n, 16]) of the last gravity pass, by data pointer."""
         poles = np.zeros((n_nodes, 24), np.float32)

@@ -266,7 +266,7 @@ sph_status sph_destroy(sph_ctx *ctx) {
     if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     void *bufs[] = {ctx->pos4, ctx->vel4, ctx->acc4, ctx->rho, ctx->u, ctx->P, ctx->h, ctx->f, ctx->c,
-                    ctx->du, ctx->B, ctx->dhdt, ctx->gnorm, ctx->mat, ctx->nat, ctx->active, ctx->globals,
+                    ctx->du, ctx->B, ctx->dhdt, ctx->gnorm, ctx->phi, ctx->mat, ctx->nat, ctx->active, ctx->globals,
                     ctx->health, ctx->cell_range, ctx->sp4, ctx->sv4, ctx->sA, ctx->sB, ctx->sC,
                     ctx->eos_forsterite, ctx->eos_fe, ctx->stage, ctx->snapshot};
     for (void *b : bufs) cudaFree(b);
@@ -328,7 +328,7 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     chk(dmalloc(&ctx->vel4, n));
     chk(dmalloc(&ctx->acc4, n));
     for (float **fp : {&ctx->rho, &ctx->u, &ctx->P, &ctx->h, &ctx->f, &ctx->c, &ctx->du, &ctx->B, &ctx->dhdt,
-                       &ctx->gnorm})
+                       &ctx->gnorm, &ctx->phi})
         chk(dmalloc(fp, n));
     chk(dmalloc(&ctx->mat, n));
     chk(dmalloc(&ctx->nat, n));
@@ -370,7 +370,7 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     ctx->eos.log_rho_range = std::log(1.f / kAneosMinRho);
     // initial state (Compute.cpp:52-77)
     chk(cudaMemset(ctx->acc4, 0, sizeof(float4) * n));
-    for (float *fp : {ctx->f, ctx->c, ctx->du, ctx->B, ctx->dhdt, ctx->gnorm})
+    for (float *fp : {ctx->f, ctx->c, ctx->du, ctx->B, ctx->dhdt, ctx->gnorm, ctx->phi})
         chk(cudaMemset(fp, 0, sizeof(float) * n));
     chk(cudaMemset(ctx->active, 1, n));
     chk(cudaMemset(ctx->nat, 0, sizeof(int32_t) * n));
@@ -535,6 +535,7 @@ sph_status sph_download(sph_ctx *ctx, sph_field field, void *host, size_t count)
         case SPH_FIELD_BALSARA: return f1(ctx->B, 4, n);
         case SPH_FIELD_DHDT: return f1(ctx->dhdt, 4, n);
         case SPH_FIELD_GRAV_NORM: return f1(ctx->gnorm, 4, n);
+        case SPH_FIELD_POTENTIAL: return f1(ctx->phi, 4, n);
         case SPH_FIELD_MATERIAL: return f1(ctx->mat, 4, n);
         case SPH_FIELD_ACTIVE: return f1(ctx->active, 1, n);
         case SPH_FIELD_NEXT_ACTIVE: return f1(ctx->nat, 4, n);
@@ -579,6 +580,7 @@ sph_status sph_get_buffer(sph_ctx *ctx, sph_field field, void **device_ptr, size
         case SPH_FIELD_BALSARA: p = ctx->B; b = 4 * n; break;
         case SPH_FIELD_DHDT: p = ctx->dhdt; b = 4 * n; break;
         case SPH_FIELD_GRAV_NORM: p = ctx->gnorm; b = 4 * n; break;
+        case SPH_FIELD_POTENTIAL: p = ctx->phi; b = 4 * n; break;
         case SPH_FIELD_MATERIAL: p = ctx->mat; b = 4 * n; break;
         case SPH_FIELD_ACTIVE: p = ctx->active; b = n; s = 1; break;
         case SPH_FIELD_NEXT_ACTIVE: p = ctx->nat; b = 4 * n; break;
@@ -754,8 +756,79 @@ sph_status sph_update_tree(sph_ctx *ctx, void *stream) {
 sph_status sph_sort(sph_ctx *ctx, void *stream) {
     return ctx ? launch_sort(ctx, (cudaStream_t)stream) : SPH_ERR_INVALID_ARG;
 }
+static sph_status gravity_pass(sph_ctx *ctx, cudaStream_t st) {
+    return ctx->form.gravity == SPH_GRAVITY_THETA ? launch_gravity_theta(ctx, st) : launch_gravity(ctx, st);
+}
 sph_status sph_gravity(sph_ctx *ctx, void *stream) {
-    return ctx ? launch_gravity(ctx, (cudaStream_t)stream) : SPH_ERR_INVALID_ARG;
+    return ctx ? gravity_pass(ctx, (cudaStream_t)stream) : SPH_ERR_INVALID_ARG;
+}
+
+void sph_form_default(sph_form *f) {
+    if (!f) return;
+    f->gravity = SPH_GRAVITY_REFERENCE;
+    f->theta = 0.5f;
+    f->h_seed = 0;
+    f->precision = 0;
+}
+
+sph_status sph_set_form(sph_ctx *ctx, const sph_form *f) {
+    if (!ctx || !f) return SPH_ERR_INVALID_ARG;
+    if (f->gravity != SPH_GRAVITY_REFERENCE && f->gravity != SPH_GRAVITY_THETA) {
+        set_error("sph_set_form: gravity = %d is not a SPH_GRAVITY_* value", (int)f->gravity);
+        return SPH_ERR_INVALID_ARG;
+    }
+    if (!(f->theta > 0.f && f->theta <= 1.5f)) {
+        set_error("sph_set_form: theta = %g is outside (0, 1.5]", (double)f->theta);
+        return SPH_ERR_INVALID_ARG;
+    }
+    if (f->h_seed != 0 || f->precision != 0) {
+        set_error("sph_set_form: h_seed and precision must be 0");
+        return SPH_ERR_UNSUPPORTED;
+    }
+    cudaSetDevice(ctx->device);
+    if (ctx->graph) {
+        cudaGraphExecDestroy(ctx->graph);
+        ctx->graph = nullptr;
+    }
+    ctx->form = *f;
+    return SPH_OK;
+}
+
+sph_status sph_get_form(const sph_ctx *ctx, sph_form *f) {
+    if (!ctx || !f) return SPH_ERR_INVALID_ARG;
+    *f = ctx->form;
+    return SPH_OK;
+}
+
+sph_status sph_gravity_direct_f64(sph_ctx *ctx, const int32_t *targets, int32_t n_targets, double *out,
+                                  void *stream) {
+    if (!ctx || n_targets < 0 || (n_targets > 0 && (!targets || !out))) return SPH_ERR_INVALID_ARG;
+    if (n_targets == 0) return SPH_OK;
+    for (int32_t t = 0; t < n_targets; ++t) {
+        if (targets[t] < 0 || targets[t] >= ctx->n) {
+            set_error("sph_gravity_direct_f64: target %d = %d is outside 0..%d", (int)t, (int)targets[t],
+                      ctx->n - 1);
+            return SPH_ERR_INVALID_ARG;
+        }
+    }
+    const size_t tgt_bytes = ((sizeof(int32_t) * (size_t)n_targets + 255) / 256) * 256;
+    const size_t out_bytes = sizeof(double) * 4 * (size_t)n_targets;
+    if (tgt_bytes + out_bytes > ctx->stage_bytes) {
+        set_error("sph_gravity_direct_f64: %d targets exceed the staging buffer (%zu bytes)", (int)n_targets,
+                  ctx->stage_bytes);
+        return SPH_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int32_t *d_t = (int32_t *)ctx->stage;
+    double *d_o = (double *)((char *)ctx->stage + tgt_bytes);
+    cudaError_t e = cudaMemcpyAsync(d_t, targets, sizeof(int32_t) * (size_t)n_targets, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e, "sph_gravity_direct_f64 upload");
+    sph_status s = launch_direct_f64(ctx, d_t, n_targets, d_o, st);
+    if (s != SPH_OK) return s;
+    e = cudaMemcpyAsync(out, d_o, out_bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return cuda_status(e, "sph_gravity_direct_f64");
 }
 sph_status sph_density(sph_ctx *ctx, void *stream) {
     return ctx ? launch_density(ctx, (cudaStream_t)stream) : SPH_ERR_INVALID_ARG;
@@ -771,7 +844,7 @@ static sph_status one_step(sph_ctx *ctx, cudaStream_t st) {
     sph_status s = SPH_OK;
     if (ctx->params.tree_source == SPH_TREE_GPU) s = launch_tree_build(ctx, st);
     if (s == SPH_OK) s = launch_sort(ctx, st);
-    if (s == SPH_OK) s = launch_gravity(ctx, st);
+    if (s == SPH_OK) s = gravity_pass(ctx, st);
     if (s == SPH_OK) s = launch_density(ctx, st);
     if (s == SPH_OK) s = launch_acceleration(ctx, st);
     if (s == SPH_OK) s = launch_step(ctx, st);

@@ -89,6 +89,8 @@ struct sph_ctx {
     float4 *pos4 = nullptr, *vel4 = nullptr, *acc4 = nullptr;
     float *rho = nullptr, *u = nullptr, *P = nullptr, *h = nullptr, *f = nullptr, *c = nullptr;
     float *du = nullptr, *B = nullptr, *dhdt = nullptr, *gnorm = nullptr;
+    float *phi = nullptr;  // potential (theta gravity form)
+    sph_form form{SPH_GRAVITY_REFERENCE, 0.5f, 0, 0};
     int32_t *mat = nullptr, *nat = nullptr;
     uint8_t *active = nullptr;
     int32_t *globals = nullptr;
@@ -139,6 +141,10 @@ sph_status launch_snapshot(sph_ctx *ctx, cudaStream_t st);
 
 // sph_gravity.cu
 sph_status launch_gravity(sph_ctx *ctx, cudaStream_t st);
+
+// sph_gravity_theta.cu
+sph_status launch_gravity_theta(sph_ctx *ctx, cudaStream_t st);
+sph_status launch_direct_f64(sph_ctx *ctx, const int32_t *d_targets, int nt, double *d_out, cudaStream_t st);
 
 // sph_tree.cu
 sph_status tree_alloc(sph_ctx *ctx);
