@@ -188,6 +188,23 @@ sph_status sph_gravity_direct_f64(sph_ctx *ctx, const int32_t *targets, int32_t 
 #define SPH_SORT_NOALLOC_MAX_N 262144
 sph_status sph_sort_cells_noalloc(const float *pos_xyz, int32_t n, uint32_t *cell_key, uint32_t *cell_index,
                                   void *stream);
+/* Health of the last sph_sort_cells_noalloc call on the current device: waits
+ * for `stream`, reads the health word kept inside the library's fixed scratch
+ * (cudaMemcpyFromSymbol, no allocation) into *word (may be NULL) and returns
+ * SPH_ERR_TIMEOUT when a bounded look-back wait gave up, in which case the
+ * call's outputs are incomplete.  The next sph_sort_cells_noalloc call clears
+ * the word.  No counterpart in the reference. */
+sph_status sph_sort_cells_noalloc_health(void *stream, uint32_t *word);
+
+/* Self-test of the radix sort's bounded look-back wait (no counterpart in the
+ * reference): one sort tile is launched whose predecessor's status words are
+ * withheld, so its wait gives up after spin_limit polls (1..2^22) and raises
+ * SPH_HEALTH_SORT_TIMEOUT without touching any key.  With ctx, the context's
+ * health word is raised (sph_synchronize then returns SPH_ERR_TIMEOUT); with
+ * ctx NULL, the allocation-free sort's (sph_sort_cells_noalloc_health then
+ * returns SPH_ERR_TIMEOUT).  The GPU stays usable; clear the word afterwards
+ * (sph_clear_health, or the next sph_sort_cells_noalloc call). */
+sph_status sph_selftest_lookback_timeout(sph_ctx *ctx, int32_t spin_limit, void *stream);
 
 /* n_steps x (tree, sort, gravity, density, acceleration, step), replayed from
  * a CUDA graph captured on first use (Headless::step without the snapshot). */
@@ -199,9 +216,19 @@ sph_status sph_step_all(sph_ctx *ctx, void *stream, int32_t n_steps);
 sph_status sph_draw_snapshot(sph_ctx *ctx, void *stream, int32_t *image);
 
 /* Buffers.hpp:14-59 (writeDataToPrivateBuffer): synchronous host<->device copies.
- * count = number of host elements (3n floats for F3 fields, n otherwise). */
+ * count = number of host elements (3n floats for F3 fields, n otherwise).
+ * They wait for all device work before and after the copy, like the
+ * reference's blit followed by waitUntilCompleted (Buffers.hpp:39-59). */
 sph_status sph_upload(sph_ctx *ctx, sph_field field, const void *host, size_t count);
 sph_status sph_download(sph_ctx *ctx, sph_field field, void *host, size_t count);
+/* The same copies ordered on `stream` and asynchronous to the host: copy,
+ * then the pack/unpack kernel of F3 and mass fields, all on `stream`, through
+ * one device staging buffer of the context (calls on one stream are ordered,
+ * so consecutive transfers may share it; do not interleave transfers of one
+ * context on two streams).  With pinned host memory the copies overlap host
+ * work; the host buffer must stay valid until the stream reaches them. */
+sph_status sph_upload_async(sph_ctx *ctx, sph_field field, const void *host, size_t count, void *stream);
+sph_status sph_download_async(sph_ctx *ctx, sph_field field, void *host, size_t count, void *stream);
 /* Borrow the device buffer behind a field (valid until sph_destroy).  F3 fields
  * are stored as 16-byte float4 records; the reported stride is in *stride. */
 sph_status sph_get_buffer(sph_ctx *ctx, sph_field field, void **device_ptr, size_t *bytes, size_t *stride);

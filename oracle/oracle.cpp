@@ -10,9 +10,10 @@
 // -ffp-contract=off so that it is bit-reproducible against the reference
 // kernels compiled through oracle/ref_shim (oracle/_ref/libref.so).
 //
-// Quirks of the reference are reproduced on purpose (Q-numbers refer to the
-// list in DESIGN.md's quirk table); the two places where the reference reads
-// out of bounds are given defined behaviour and say so.
+// Quirks of the reference are reproduced on purpose (each one is described
+// where it occurs, with the reference line it comes from); the two places
+// where the reference reads out of bounds are given defined behaviour and say
+// so.
 
 #include "oracle.h"
 

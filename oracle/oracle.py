@@ -56,8 +56,15 @@ def build(force: bool = False) -> str:
     return LIB_PATH
 
 
-def build_ref(reference_root: str = "/root/reference") -> str | None:
+def reference_root() -> str:
+    """Root of the reference checkout: $SPH_REFERENCE_ROOT, else the path the
+    build recipe (ref_build.sh) defaults to."""
+    return os.environ.get("SPH_REFERENCE_ROOT", "/root/reference")
+
+
+def build_ref(reference_root_dir: str | None = None) -> str | None:
     """Build _ref/libref.so from the reference's sources when they are present."""
+    reference_root = reference_root_dir or globals()["reference_root"]()
     if not os.path.isdir(os.path.join(reference_root, "SPH", "Shaders")):
         return None
     subprocess.run([os.path.join(HERE, "ref_build.sh"), reference_root], check=True,

@@ -234,6 +234,22 @@ class Compute:
         _lib.check(self._lib.sph_upload(self._h, _lib.FIELDS[field], a.ctypes.data_as(C.c_void_p), a.size),
                    f"sph_upload({field})")
 
+    def upload_async(self, field: str, values: np.ndarray, stream=None) -> None:
+        """Stream-ordered upload from a caller-held host array (pinned for
+        overlap); the array must stay alive until the stream reaches the copy."""
+        if not values.flags.c_contiguous:
+            raise ValueError("upload_async needs a C-contiguous array")
+        _lib.check(self._lib.sph_upload_async(self._h, _lib.FIELDS[field], values.ctypes.data_as(C.c_void_p),
+                                              values.size, _stream(stream)), f"sph_upload_async({field})")
+
+    def download_async(self, field: str, out: np.ndarray, stream=None) -> None:
+        """Stream-ordered download into a caller-held host array (pinned for
+        overlap); valid once the stream has been synchronised."""
+        if not out.flags.c_contiguous:
+            raise ValueError("download_async needs a C-contiguous array")
+        _lib.check(self._lib.sph_download_async(self._h, _lib.FIELDS[field], out.ctypes.data_as(C.c_void_p),
+                                                out.size, _stream(stream)), f"sph_download_async({field})")
+
     def device_buffer(self, field: str):
         """(device pointer, bytes, stride) of a field's storage."""
         p, b, s = C.c_void_p(), C.c_size_t(), C.c_size_t()

@@ -405,21 +405,21 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     return SPH_OK;
 }
 
-sph_status sph_upload(sph_ctx *ctx, sph_field field, const void *host, size_t count) {
+sph_status sph_upload_async(sph_ctx *ctx, sph_field field, const void *host, size_t count, void *stream) {
     if (!ctx || !host) {
         set_error("sph_upload: null argument");
         return SPH_ERR_INVALID_ARG;
     }
     const int n = ctx->n;
     const size_t need3 = 3 * (size_t)n, need1 = (size_t)n;
-    cudaError_t e = cudaSuccess;
+    cudaStream_t st = (cudaStream_t)stream;
     const int blocks = (n + 255) / 256;
     auto f1 = [&](void *dst, size_t elem) -> sph_status {
         if (count != need1) {
             set_error("sph_upload: field %d expects %zu elements, got %zu", (int)field, need1, count);
             return SPH_ERR_INVALID_ARG;
         }
-        return cuda_status(cudaMemcpy(dst, host, elem * count, cudaMemcpyHostToDevice), "sph_upload");
+        return cuda_status(cudaMemcpyAsync(dst, host, elem * count, cudaMemcpyHostToDevice, st), "sph_upload");
     };
     switch (field) {
         case SPH_FIELD_POS:
@@ -430,10 +430,10 @@ sph_status sph_upload(sph_ctx *ctx, sph_field field, const void *host, size_t co
                 return SPH_ERR_INVALID_ARG;
             }
             float4 *dst = field == SPH_FIELD_POS ? ctx->pos4 : field == SPH_FIELD_VEL ? ctx->vel4 : ctx->acc4;
-            e = cudaMemcpy(ctx->stage, host, sizeof(float) * count, cudaMemcpyHostToDevice);
+            cudaError_t e = cudaMemcpyAsync(ctx->stage, host, sizeof(float) * count, cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess) {
-                k_pack3<<<blocks, 256>>>((const float *)ctx->stage, dst, n, field == SPH_FIELD_POS ? 1 : 0);
-                e = cudaDeviceSynchronize();
+                k_pack3<<<blocks, 256, 0, st>>>((const float *)ctx->stage, dst, n, field == SPH_FIELD_POS ? 1 : 0);
+                e = cudaGetLastError();
             }
             return cuda_status(e, "sph_upload");
         }
@@ -442,10 +442,10 @@ sph_status sph_upload(sph_ctx *ctx, sph_field field, const void *host, size_t co
                 set_error("sph_upload: mass expects %zu floats", need1);
                 return SPH_ERR_INVALID_ARG;
             }
-            e = cudaMemcpy(ctx->stage, host, sizeof(float) * count, cudaMemcpyHostToDevice);
+            cudaError_t e = cudaMemcpyAsync(ctx->stage, host, sizeof(float) * count, cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess) {
-                k_set_w<<<blocks, 256>>>((const float *)ctx->stage, ctx->pos4, n);
-                e = cudaDeviceSynchronize();
+                k_set_w<<<blocks, 256, 0, st>>>((const float *)ctx->stage, ctx->pos4, n);
+                e = cudaGetLastError();
             }
             return cuda_status(e, "sph_upload");
         }
@@ -479,8 +479,8 @@ sph_status sph_upload(sph_ctx *ctx, sph_field field, const void *host, size_t co
                 set_error("sph_upload: scalar field expects 1 element");
                 return SPH_ERR_INVALID_ARG;
             }
-            return cuda_status(cudaMemcpy(ctx->globals + (field == SPH_FIELD_DT ? 1 : 0), host, 4,
-                                          cudaMemcpyHostToDevice),
+            return cuda_status(cudaMemcpyAsync(ctx->globals + (field == SPH_FIELD_DT ? 1 : 0), host, 4,
+                                               cudaMemcpyHostToDevice, st),
                                "sph_upload");
         default:
             set_error("sph_upload: field %d is read-only", (int)field);
@@ -488,21 +488,30 @@ sph_status sph_upload(sph_ctx *ctx, sph_field field, const void *host, size_t co
     }
 }
 
-sph_status sph_download(sph_ctx *ctx, sph_field field, void *host, size_t count) {
+sph_status sph_upload(sph_ctx *ctx, sph_field field, const void *host, size_t count) {
+    if (!ctx) return SPH_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_status(e, "sph_upload");
+    sph_status s = sph_upload_async(ctx, field, host, count, nullptr);
+    if (s != SPH_OK) return s;
+    return cuda_status(cudaDeviceSynchronize(), "sph_upload");
+}
+
+sph_status sph_download_async(sph_ctx *ctx, sph_field field, void *host, size_t count, void *stream) {
     if (!ctx || !host) {
         set_error("sph_download: null argument");
         return SPH_ERR_INVALID_ARG;
     }
     const int n = ctx->n;
     const int blocks = (n + 255) / 256;
-    cudaError_t e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) return cuda_status(e, "sph_download");
+    cudaStream_t st = (cudaStream_t)stream;
     auto f1 = [&](const void *src, size_t elem, size_t need) -> sph_status {
         if (count != need) {
             set_error("sph_download: field %d expects %zu elements, got %zu", (int)field, need, count);
             return SPH_ERR_INVALID_ARG;
         }
-        return cuda_status(cudaMemcpy(host, src, elem * count, cudaMemcpyDeviceToHost), "sph_download");
+        return cuda_status(cudaMemcpyAsync(host, src, elem * count, cudaMemcpyDeviceToHost, st), "sph_download");
     };
     switch (field) {
         case SPH_FIELD_POS:
@@ -513,17 +522,17 @@ sph_status sph_download(sph_ctx *ctx, sph_field field, void *host, size_t count)
                 return SPH_ERR_INVALID_ARG;
             }
             const float4 *src = field == SPH_FIELD_POS ? ctx->pos4 : field == SPH_FIELD_VEL ? ctx->vel4 : ctx->acc4;
-            k_unpack3<<<blocks, 256>>>(src, (float *)ctx->stage, n);
-            e = cudaMemcpy(host, ctx->stage, sizeof(float) * count, cudaMemcpyDeviceToHost);
-            return cuda_status(e, "sph_download");
+            k_unpack3<<<blocks, 256, 0, st>>>(src, (float *)ctx->stage, n);
+            return cuda_status(cudaMemcpyAsync(host, ctx->stage, sizeof(float) * count, cudaMemcpyDeviceToHost, st),
+                               "sph_download");
         }
         case SPH_FIELD_MASS:
             if (count != (size_t)n) {
                 set_error("sph_download: mass expects %d floats", n);
                 return SPH_ERR_INVALID_ARG;
             }
-            k_get_w<<<blocks, 256>>>(ctx->pos4, (float *)ctx->stage, n);
-            return cuda_status(cudaMemcpy(host, ctx->stage, sizeof(float) * n, cudaMemcpyDeviceToHost),
+            k_get_w<<<blocks, 256, 0, st>>>(ctx->pos4, (float *)ctx->stage, n);
+            return cuda_status(cudaMemcpyAsync(host, ctx->stage, sizeof(float) * n, cudaMemcpyDeviceToHost, st),
                                "sph_download");
         case SPH_FIELD_RHO: return f1(ctx->rho, 4, n);
         case SPH_FIELD_U: return f1(ctx->u, 4, n);
@@ -549,15 +558,26 @@ sph_status sph_download(sph_ctx *ctx, sph_field field, void *host, size_t count)
                 set_error("sph_download: cell tables hold %u entries", kNumCells);
                 return SPH_ERR_INVALID_ARG;
             }
-            k_split_cells<<<148 * 8, 256>>>(ctx->cell_range, (uint32_t *)ctx->stage, kNumCells,
-                                            field == SPH_FIELD_CELL_END ? 1 : 0);
-            return cuda_status(cudaMemcpy(host, ctx->stage, sizeof(uint32_t) * kNumCells, cudaMemcpyDeviceToHost),
-                               "sph_download");
+            k_split_cells<<<148 * 8, 256, 0, st>>>(ctx->cell_range, (uint32_t *)ctx->stage, kNumCells,
+                                                   field == SPH_FIELD_CELL_END ? 1 : 0);
+            return cuda_status(
+                cudaMemcpyAsync(host, ctx->stage, sizeof(uint32_t) * kNumCells, cudaMemcpyDeviceToHost, st),
+                "sph_download");
         }
         default:
             set_error("sph_download: unknown field %d", (int)field);
             return SPH_ERR_INVALID_ARG;
     }
+}
+
+sph_status sph_download(sph_ctx *ctx, sph_field field, void *host, size_t count) {
+    if (!ctx) return SPH_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_status(e, "sph_download");
+    sph_status s = sph_download_async(ctx, field, host, count, nullptr);
+    if (s != SPH_OK) return s;
+    return cuda_status(cudaDeviceSynchronize(), "sph_download");
 }
 
 sph_status sph_get_buffer(sph_ctx *ctx, sph_field field, void **device_ptr, size_t *bytes, size_t *stride) {

@@ -33,6 +33,7 @@ struct RadixSorter {
     uint32_t *counters = nullptr; // [kMaxPasses] tile tickets
     int n_cap = 0;
     int tiles_cap = 0;
+    int spin_limit = 1 << 22;     // polls before a look-back wait gives up
     static constexpr int kThreads = 256;
     static constexpr int kItems = 16;
     static constexpr int kTile = kThreads * kItems;

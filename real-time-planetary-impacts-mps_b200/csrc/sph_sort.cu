@@ -20,7 +20,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
 
 #include "sph_internal.h"
 
@@ -72,7 +71,8 @@ __global__ void k_hash_hist(const float4 *__restrict__ pos4, int n, uint32_t *__
 __global__ void __launch_bounds__(RadixSorter::kThreads)
     k_onesweep(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int n, int shift,
-               const uint32_t *__restrict__ hist, uint32_t *status, uint32_t *counter, uint32_t *health) {
+               const uint32_t *__restrict__ hist, uint32_t *status, uint32_t *counter, uint32_t *health,
+               int spin_limit) {
     constexpr int T = RadixSorter::kThreads, I = RadixSorter::kItems, W = T / 32;
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp[W][256];
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(RadixSorter::kThreads)
             uint32_t s = vs[(size_t)j * 256 + tid];
             uint32_t flag = s & ~kValueMask;
             if (flag == 0u) {
-                if (++spins > kSpinLimit) {
+                if (++spins > spin_limit) {
                     raise_health(health, SPH_HEALTH_SORT_TIMEOUT);
                     break;
                 }
@@ -319,7 +319,7 @@ int radix_sort_pairs(RadixSorter &s, int n, int bits, cudaStream_t st, uint32_t 
         k_onesweep<<<tiles, RadixSorter::kThreads, 0, st>>>(s.keys[cur], s.vals[cur], s.keys[cur ^ 1],
                                                              s.vals[cur ^ 1], n, 8 * p, s.hist + 256 * p,
                                                              s.status + (size_t)256 * tiles * p, s.counters + p,
-                                                             health);
+                                                             health, s.spin_limit);
         cur ^= 1;
     }
     return cur;
@@ -371,12 +371,16 @@ sph_status launch_sort(sph_ctx *ctx, cudaStream_t st) {
 // The scratch is a file-scope __device__ array, so every GPU that loads the
 // library carries it (kNoAllocScratchBytes, about 2.2 MiB) until the process
 // exits.  On the host, the array's name is only a stand-in symbol, not a
-// device address; its device address is looked up once per device with
-// cudaGetSymbolAddress, on the first call made while that device is current.
-// Every call shares the array and it keeps the last call's contents, so the
-// parts that must start at zero are cleared on the caller's stream at each
-// call, and calls whose work overlaps on the GPU (different streams without
-// ordering, or several host threads) race on it.
+// device address; its device address is looked up with cudaGetSymbolAddress
+// on every call, for the device current at that call (the first lookup on a
+// device loads the module there, which is why the first call should come
+// before any stream capture).  Every call shares the array and it keeps the
+// last call's contents, so the parts that must start at zero (histograms,
+// tile tickets, the health word and the look-back words this call's size
+// uses) are cleared on the caller's stream at each call, and calls whose work
+// overlaps on the GPU (different streams without ordering, or several host
+// threads) race on it.  A look-back wait that gives up raises the health word
+// inside the scratch; sph_sort_cells_noalloc_health reads it back.
 // ---------------------------------------------------------------------------
 namespace sph {
 namespace {
@@ -385,20 +389,16 @@ constexpr int kNoAllocPasses = 3;  // 24-bit cell keys
 constexpr int kNoAllocTiles = (SPH_SORT_NOALLOC_MAX_N + RadixSorter::kTile - 1) / RadixSorter::kTile;
 constexpr size_t kNoAllocKeysOff = 0;
 constexpr size_t kNoAllocValsOff = kNoAllocKeysOff + sizeof(uint32_t) * SPH_SORT_NOALLOC_MAX_N;
+// the words that must be zero when a call starts sit together from here on:
+// histograms, tile tickets, the health word, then the look-back words of the
+// three passes, each pass using 256 x (tiles of this call) words
 constexpr size_t kNoAllocHistOff = kNoAllocValsOff + sizeof(uint32_t) * SPH_SORT_NOALLOC_MAX_N;
-constexpr size_t kNoAllocStatusOff = kNoAllocHistOff + sizeof(uint32_t) * 256 * kNoAllocPasses;
-constexpr size_t kNoAllocCountOff = kNoAllocStatusOff + sizeof(uint32_t) * 256 * kNoAllocTiles * kNoAllocPasses;
+constexpr size_t kNoAllocCountOff = kNoAllocHistOff + sizeof(uint32_t) * 256 * kNoAllocPasses;
 constexpr size_t kNoAllocHealthOff = kNoAllocCountOff + sizeof(uint32_t) * kNoAllocPasses;
-constexpr size_t kNoAllocScratchBytes = kNoAllocHealthOff + sizeof(uint32_t);
-// bytes that must be zero when a call starts: histograms, look-back words,
-// tile tickets and the health word
-constexpr size_t kNoAllocZeroBytes = kNoAllocScratchBytes - kNoAllocHistOff;
+constexpr size_t kNoAllocStatusOff = kNoAllocHealthOff + sizeof(uint32_t);
+constexpr size_t kNoAllocScratchBytes = kNoAllocStatusOff + sizeof(uint32_t) * 256 * kNoAllocTiles * kNoAllocPasses;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
-
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-unsigned char *g_noalloc_dev[kNoAllocMaxDevices] = {};
 
 // sort.metal:15-44 from xyz-interleaved positions, plus the digit histograms
 // of the three passes (same keys as k_hash_hist; no cell table to clear).
@@ -422,23 +422,12 @@ __global__ void k_hash_hist_xyz(const float *__restrict__ pos, int n, uint32_t *
     }
 }
 
-// Device address of the scratch array on the current device (set-up on first use).
+// Device address of the scratch array on the current device.
 sph_status noalloc_scratch(unsigned char **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_status(e, "sph_sort_cells_noalloc: cudaGetDevice");
-    if (dev < 0 || dev >= kNoAllocMaxDevices) {
-        set_error("sph_sort_cells_noalloc: device ordinal %d is not supported", dev);
-        return SPH_ERR_UNSUPPORTED;
-    }
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_dev[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_status(e, "sph_sort_cells_noalloc: cudaGetSymbolAddress");
-        g_noalloc_dev[dev] = static_cast<unsigned char *>(p);
-    }
-    *out = g_noalloc_dev[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_status(e, "sph_sort_cells_noalloc: cudaGetSymbolAddress");
+    *out = static_cast<unsigned char *>(p);
     return SPH_OK;
 }
 
@@ -463,26 +452,99 @@ extern "C" sph_status sph_sort_cells_noalloc(const float *pos_xyz, int32_t n, ui
     sph_status st = noalloc_scratch(&s);
     if (st != SPH_OK) return st;
     cudaStream_t cs = (cudaStream_t)stream;
+    const int tiles = (n + RadixSorter::kTile - 1) / RadixSorter::kTile;
     uint32_t *tk = reinterpret_cast<uint32_t *>(s + kNoAllocKeysOff);
     uint32_t *tv = reinterpret_cast<uint32_t *>(s + kNoAllocValsOff);
     uint32_t *hist = reinterpret_cast<uint32_t *>(s + kNoAllocHistOff);
-    uint32_t *status = reinterpret_cast<uint32_t *>(s + kNoAllocStatusOff);
     uint32_t *counters = reinterpret_cast<uint32_t *>(s + kNoAllocCountOff);
     uint32_t *health = reinterpret_cast<uint32_t *>(s + kNoAllocHealthOff);
-    cudaError_t e = cudaMemsetAsync(s + kNoAllocHistOff, 0, kNoAllocZeroBytes, cs);
+    uint32_t *status = reinterpret_cast<uint32_t *>(s + kNoAllocStatusOff);
+    const size_t zero_bytes = (kNoAllocStatusOff - kNoAllocHistOff) + sizeof(uint32_t) * 256 * (size_t)tiles * kNoAllocPasses;
+    cudaError_t e = cudaMemsetAsync(s + kNoAllocHistOff, 0, zero_bytes, cs);
     if (e != cudaSuccess) return cuda_status(e, "sph_sort_cells_noalloc: clear scratch");
     int blocks = (n + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
     k_hash_hist_xyz<<<blocks, 256, 0, cs>>>(pos_xyz, n, tk, tv, hist);
     // three stable 8-bit passes: scratch -> out -> scratch -> out
-    const int tiles = (n + RadixSorter::kTile - 1) / RadixSorter::kTile;
     uint32_t *kin[kNoAllocPasses] = {tk, cell_key, tk};
     uint32_t *vin[kNoAllocPasses] = {tv, cell_index, tv};
     uint32_t *kout[kNoAllocPasses] = {cell_key, tk, cell_key};
     uint32_t *vout[kNoAllocPasses] = {cell_index, tv, cell_index};
     for (int p = 0; p < kNoAllocPasses; ++p)
         k_onesweep<<<tiles, RadixSorter::kThreads, 0, cs>>>(kin[p], vin[p], kout[p], vout[p], n, 8 * p, hist + 256 * p,
-                                                            status + (size_t)256 * kNoAllocTiles * p, counters + p,
-                                                            health);
+                                                            status + (size_t)256 * tiles * p, counters + p, health,
+                                                            kSpinLimit);
     return cuda_status(cudaGetLastError(), "sph_sort_cells_noalloc");
+}
+
+extern "C" sph_status sph_sort_cells_noalloc_health(void *stream, uint32_t *word) {
+    using namespace sph;
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_status(e, "sph_sort_cells_noalloc_health: stream");
+    uint32_t w = 0;
+    e = cudaMemcpyFromSymbol(&w, g_noalloc_scratch, sizeof(uint32_t), kNoAllocHealthOff, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e, "sph_sort_cells_noalloc_health: read");
+    if (word) *word = w;
+    if (w & SPH_HEALTH_SORT_TIMEOUT) {
+        set_error("sph_sort_cells_noalloc: a look-back wait gave up (health 0x%x); the outputs are incomplete", w);
+        return SPH_ERR_TIMEOUT;
+    }
+    return SPH_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded look-back wait.  One k_onesweep tile is launched
+// whose ticket is preset to 1, so it waits on tile 0's status words, which
+// nothing writes: the wait must give up after spin_limit polls, raise
+// SPH_HEALTH_SORT_TIMEOUT and return.  The tile holds no elements (n = 0), so
+// it reads and writes no key or value.  With ctx the context's sorter scratch
+// and health word are used (sph_synchronize then reports SPH_ERR_TIMEOUT);
+// without, the allocation-free sort's static scratch is used
+// (sph_sort_cells_noalloc_health then reports it).
+// ---------------------------------------------------------------------------
+namespace sph {
+namespace {
+__global__ void k_selftest_prepare(uint32_t *hist, uint32_t *status, uint32_t *counter) {
+    const int t = threadIdx.x;  // 256 threads
+    hist[t] = 0u;
+    status[t] = 0u;
+    status[256 + t] = 0u;
+    if (t == 0) *counter = 1u;
+}
+}  // namespace
+}  // namespace sph
+
+extern "C" sph_status sph_selftest_lookback_timeout(sph_ctx *ctx, int32_t spin_limit, void *stream) {
+    using namespace sph;
+    if (spin_limit < 1 || spin_limit > (1 << 22)) {
+        set_error("sph_selftest_lookback_timeout: spin_limit %d is outside 1..%d", spin_limit, 1 << 22);
+        return SPH_ERR_INVALID_ARG;
+    }
+    cudaStream_t cs = (cudaStream_t)stream;
+    uint32_t *hist, *status, *counter, *health, *kbuf, *vbuf;
+    if (ctx) {
+        cudaSetDevice(ctx->device);
+        RadixSorter &r = ctx->cell_sort;  // status holds >= 4 x 256 words
+        hist = r.hist;
+        status = r.status;
+        counter = r.counters;
+        health = ctx->health;
+        kbuf = r.keys[0];
+        vbuf = r.vals[0];
+    } else {
+        unsigned char *s = nullptr;
+        sph_status st = noalloc_scratch(&s);
+        if (st != SPH_OK) return st;
+        hist = reinterpret_cast<uint32_t *>(s + kNoAllocHistOff);
+        counter = reinterpret_cast<uint32_t *>(s + kNoAllocCountOff);
+        health = reinterpret_cast<uint32_t *>(s + kNoAllocHealthOff);
+        status = reinterpret_cast<uint32_t *>(s + kNoAllocStatusOff);
+        kbuf = reinterpret_cast<uint32_t *>(s + kNoAllocKeysOff);
+        vbuf = reinterpret_cast<uint32_t *>(s + kNoAllocValsOff);
+    }
+    // the key/value buffers are valid device memory, though n = 0 touches none
+    k_selftest_prepare<<<1, 256, 0, cs>>>(hist, status, counter);
+    k_onesweep<<<1, RadixSorter::kThreads, 0, cs>>>(kbuf, vbuf, kbuf, vbuf, 0, 0, hist, status, counter,
+                                                    health, spin_limit);
+    return cuda_status(cudaGetLastError(), "sph_selftest_lookback_timeout");
 }

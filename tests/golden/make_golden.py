@@ -6,7 +6,7 @@ oracle/ref_build.sh compiles its Metal kernels (SPH/Shaders/*.metal, through a
 host shim), its CPU octree (SPH/octree/octree.cpp) and its ANEOS loader
 (SPH/ANEOS/ANEOS.cpp) unchanged into oracle/_ref/libref.so, and this script
 drives them in the dispatch order of SPH/Compute/Compute.cpp on seeded
-synthetic inputs.  Needs the reference tree (default /root/reference); the
+synthetic inputs.  Needs the reference tree ($SPH_REFERENCE_ROOT, default the recipe's path); the
 fixtures are committed so the tests run without it.
 
     python tests/golden/make_golden.py [reference_root]
@@ -43,7 +43,8 @@ def occupied_cells(st) -> np.ndarray:
     return np.stack([occ, st.cell_start[occ], st.cell_end[occ]], axis=1)
 
 
-def main(ref_root: str = "/root/reference"):
+def main(ref_root: str | None = None):
+    ref_root = ref_root or O.reference_root()
     if O.build_ref(ref_root) is None:
         raise SystemExit(f"reference sources not found under {ref_root}")
     O.build()
