@@ -13,6 +13,11 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "libsph_b200.so")
+# The parity build: the same sources with FMA contraction off (-fmad=false)
+# and SPH_PARITY, under which every float sum runs in the reference's
+# sequential order.  Only the parity tests load it; it is not the product.
+PARITY_LIB_PATH = os.path.join(HERE, "libsph_b200_parity.so")
+PARITY_FLAGS = ["-fmad=false", "-DSPH_PARITY"]
 SOURCES = ["sph_api.cu", "sph_sort.cu", "sph_hydro.cu", "sph_gravity.cu", "sph_gravity_theta.cu", "sph_tree.cu"]
 HEADERS = ["sph_common.cuh", "sph_internal.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
@@ -74,38 +79,61 @@ class SphError(RuntimeError):
         super().__init__(f"{what}: {STATUS.get(status, status)}" + (f" ({detail})" if detail else ""))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile libsph_b200.so for sm_100a in place (cross-compiles without a GPU)."""
+def build(force: bool = False, verbose: bool = False, parity: bool = False) -> str:
+    """Compile libsph_b200.so (or, with parity=True, libsph_b200_parity.so)
+    for sm_100a in place (cross-compiles without a GPU).  The sources are
+    compiled in parallel and linked into one shared library."""
+    from concurrent.futures import ThreadPoolExecutor
+    out = PARITY_LIB_PATH if parity else LIB_PATH
     csrc = os.path.join(HERE, "csrc")
     srcs = [os.path.join(csrc, s) for s in SOURCES]
     deps = srcs + [os.path.join(csrc, h) for h in HEADERS] + [os.path.join(ROOT, "include", "sph.h")]
-    if not force and os.path.exists(LIB_PATH):
-        t = os.path.getmtime(LIB_PATH)
+    if not force and os.path.exists(out):
+        t = os.path.getmtime(out)
         if all(os.path.getmtime(d) <= t for d in deps):
-            return LIB_PATH
+            return out
     nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
     if not os.path.exists(nvcc):
         nvcc = "nvcc"
-    tmp = LIB_PATH + f".{os.getpid()}.tmp"
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", tmp] + srcs
-    res = subprocess.run(cmd, capture_output=not verbose, text=True)
-    if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + (res.stderr or "") + (res.stdout or ""))
-    os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+    flags = NVCC_FLAGS[:-1] + (PARITY_FLAGS if parity else [])  # without -shared for the objects
+    tag = f"{os.getpid()}{'p' if parity else ''}"
+    objs = [out + f".{os.path.basename(s)}.{tag}.o" for s in srcs]
+
+    def compile_one(pair):
+        src, obj = pair
+        return subprocess.run([nvcc] + flags + ["-c", "-o", obj, src], capture_output=not verbose, text=True)
+
+    with ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+        results = list(ex.map(compile_one, zip(srcs, objs)))
+    try:
+        for r in results:
+            if r.returncode != 0:
+                raise RuntimeError("nvcc failed:\n" + (r.stderr or "") + (r.stdout or ""))
+        tmp = out + f".{tag}.tmp"
+        r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp] + objs,
+                           capture_output=not verbose, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc link failed:\n" + (r.stderr or "") + (r.stdout or ""))
+        os.replace(tmp, out)
+    finally:
+        for o in objs:
+            if os.path.exists(o):
+                os.remove(o)
+    return out
 
 
-_LIB = None
+_LIBS: dict = {}
 
 
-def load() -> C.CDLL:
-    """Load the CUDA library (built in place).  Raises if it is missing."""
-    global _LIB
-    if _LIB is not None:
-        return _LIB
-    if not os.path.exists(LIB_PATH):
-        raise FileNotFoundError(f"{LIB_PATH} is not built; run __graft_entry__.build()")
-    lib = C.CDLL(LIB_PATH)
+def load(parity: bool = False) -> C.CDLL:
+    """Load the CUDA library (built in place), or its parity build.  Raises if
+    it is missing."""
+    if parity in _LIBS:
+        return _LIBS[parity]
+    path = PARITY_LIB_PATH if parity else LIB_PATH
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built; run __graft_entry__.build()")
+    lib = C.CDLL(path)
     vp = C.c_void_p
     st = C.c_int
     sig = {
@@ -147,13 +175,13 @@ def load() -> C.CDLL:
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
-    _LIB = lib
+    _LIBS[parity] = lib
     return lib
 
 
-def check(status: int, what: str):
+def check(status: int, what: str, lib: C.CDLL | None = None):
     if status != SPH_OK:
-        detail = load().sph_last_error().decode(errors="replace")
+        detail = (lib or load()).sph_last_error().decode(errors="replace")
         raise SphError(status, what, detail)
 
 

@@ -47,8 +47,11 @@ class Compute:
     def __init__(self, ic: dict, *, max_children_in_leaf: int = 4, max_tree_depth: int = 7,
                  max_unchecked_pointers: int = 1024, aneos_resolution: int = 2048,
                  tree_source: str = "gpu", forsterite_table: str | None = None,
-                 fe85si15_table: str | None = None):
-        lib = _lib.load()
+                 fe85si15_table: str | None = None, parity: bool = False):
+        # parity=True runs the parity build (no FMA contraction, sums in the
+        # reference's sequential order); only tests use it
+        lib = _lib.load(parity)
+        self._lib = lib
         if forsterite_table is None or fe85si15_table is None:
             tabs = eos_tables.ensure_tables()
             forsterite_table = forsterite_table or tabs["forsterite"]
@@ -76,11 +79,14 @@ class Compute:
             setattr(s, k, _ptr(keep[k], _fp))
         s.material = _ptr(keep["material"], _ip)
         h = C.c_void_p()
-        _lib.check(lib.sph_create(C.byref(p), C.byref(s), C.byref(h)), "sph_create")
+        _lib.check(lib.sph_create(C.byref(p), C.byref(s), C.byref(h)), "sph_create", lib)
         self._lib = lib
         self._h = h
         self.nParticles = n
         self.tree_source = tree_source
+
+    def _check(self, status: int, what: str):
+        _lib.check(status, what, self._lib)
 
     # ---- lifetime ------------------------------------------------------
     def close(self):
@@ -102,29 +108,29 @@ class Compute:
 
     # ---- passes (Headless.cpp:43-51 order) -----------------------------
     def updateOctreeBuffer(self, stream=None):
-        _lib.check(self._lib.sph_update_tree(self._h, _stream(stream)), "sph_update_tree")
+        self._check(self._lib.sph_update_tree(self._h, _stream(stream)), "sph_update_tree")
 
     def sort(self, stream=None):
-        _lib.check(self._lib.sph_sort(self._h, _stream(stream)), "sph_sort")
+        self._check(self._lib.sph_sort(self._h, _stream(stream)), "sph_sort")
 
     def gravitationalPass(self, stream=None):
-        _lib.check(self._lib.sph_gravity(self._h, _stream(stream)), "sph_gravity")
+        self._check(self._lib.sph_gravity(self._h, _stream(stream)), "sph_gravity")
 
     def densityPass(self, stream=None):
-        _lib.check(self._lib.sph_density(self._h, _stream(stream)), "sph_density")
+        self._check(self._lib.sph_density(self._h, _stream(stream)), "sph_density")
 
     def accelerationPass(self, stream=None):
-        _lib.check(self._lib.sph_acceleration(self._h, _stream(stream)), "sph_acceleration")
+        self._check(self._lib.sph_acceleration(self._h, _stream(stream)), "sph_acceleration")
 
     def stepPass(self, stream=None):
-        _lib.check(self._lib.sph_step(self._h, _stream(stream)), "sph_step")
+        self._check(self._lib.sph_step(self._h, _stream(stream)), "sph_step")
 
     def drawSnapshot(self, stream=None, download: bool = True):
         if not download:
-            _lib.check(self._lib.sph_draw_snapshot(self._h, _stream(stream), None), "sph_draw_snapshot")
+            self._check(self._lib.sph_draw_snapshot(self._h, _stream(stream), None), "sph_draw_snapshot")
             return None
         img = np.zeros((1024, 1024), np.int32)
-        _lib.check(self._lib.sph_draw_snapshot(self._h, _stream(stream), _ptr(img, _ip)), "sph_draw_snapshot")
+        self._check(self._lib.sph_draw_snapshot(self._h, _stream(stream), _ptr(img, _ip)), "sph_draw_snapshot")
         return img
 
     def step(self, stream=None):
@@ -139,10 +145,10 @@ class Compute:
 
     def step_all(self, n_steps: int, stream=None):
         """n_steps full steps replayed from a captured CUDA graph."""
-        _lib.check(self._lib.sph_step_all(self._h, _stream(stream), int(n_steps)), "sph_step_all")
+        self._check(self._lib.sph_step_all(self._h, _stream(stream), int(n_steps)), "sph_step_all")
 
     def synchronize(self, stream=None):
-        _lib.check(self._lib.sph_synchronize(self._h, _stream(stream)), "sph_synchronize")
+        self._check(self._lib.sph_synchronize(self._h, _stream(stream)), "sph_synchronize")
 
     # ---- trees ---------------------------------------------------------
     def set_tree(self, tree: dict):
@@ -151,7 +157,7 @@ class Compute:
         t = np.ascontiguousarray(tree["tree"], np.int32)
         off = np.ascontiguousarray(tree["level_offsets"], np.int32)
         nodes = np.ascontiguousarray(tree["level_nodes"], np.int32)
-        _lib.check(self._lib.sph_set_tree(self._h, _ptr(t, _ip), int(t.shape[0]), _ptr(off, _ip),
+        self._check(self._lib.sph_set_tree(self._h, _ptr(t, _ip), int(t.shape[0]), _ptr(off, _ip),
                                           _ptr(nodes, _ip), int(tree["n_levels"]), int(tree["n_nodes"])),
                    "sph_set_tree")
         self.tree_source = "host"
@@ -159,12 +165,12 @@ class Compute:
     def get_tree(self) -> dict:
         """The current tree in the reference format (synchronous)."""
         ln, nl, nn = C.c_int32(), C.c_int32(), C.c_int32()
-        _lib.check(self._lib.sph_get_tree(self._h, None, 0, C.byref(ln), None, None, 0, C.byref(nl), C.byref(nn)),
+        self._check(self._lib.sph_get_tree(self._h, None, 0, C.byref(ln), None, None, 0, C.byref(nl), C.byref(nn)),
                    "sph_get_tree")
         tree = np.zeros(max(ln.value, 1), np.int32)
         off = np.zeros(17, np.int32)
         nodes = np.zeros(max(nn.value, 1), np.int32)
-        _lib.check(self._lib.sph_get_tree(self._h, _ptr(tree, _ip), tree.size, C.byref(ln), _ptr(off, _ip),
+        self._check(self._lib.sph_get_tree(self._h, _ptr(tree, _ip), tree.size, C.byref(ln), _ptr(off, _ip),
                                           _ptr(nodes, _ip), nodes.size, C.byref(nl), C.byref(nn)), "sph_get_tree")
         return dict(tree=tree[:ln.value], level_offsets=off[:nl.value + 1], level_nodes=nodes[:off[nl.value]],
                     n_levels=nl.value, n_nodes=nn.value)
@@ -177,18 +183,18 @@ class Compute:
         self._lib.sph_form_default(C.byref(f))
         f.gravity = _lib.SPH_GRAVITY_THETA if gravity == "theta" else _lib.SPH_GRAVITY_REFERENCE
         f.theta = float(theta)
-        _lib.check(self._lib.sph_set_form(self._h, C.byref(f)), "sph_set_form")
+        self._check(self._lib.sph_set_form(self._h, C.byref(f)), "sph_set_form")
 
     def get_form(self) -> dict:
         f = _lib.SphForm()
-        _lib.check(self._lib.sph_get_form(self._h, C.byref(f)), "sph_get_form")
+        self._check(self._lib.sph_get_form(self._h, C.byref(f)), "sph_get_form")
         return dict(gravity="theta" if f.gravity == _lib.SPH_GRAVITY_THETA else "reference", theta=f.theta)
 
     def gravity_direct_f64(self, targets, stream=None) -> np.ndarray:
         """FP64 direct-sum (ax, ay, az, phi) at the given particles, G included."""
         t = np.ascontiguousarray(np.asarray(targets, np.int32).reshape(-1))
         out = np.zeros((t.size, 4), np.float64)
-        _lib.check(self._lib.sph_gravity_direct_f64(self._h, _ptr(t, _ip), int(t.size),
+        self._check(self._lib.sph_gravity_direct_f64(self._h, _ptr(t, _ip), int(t.size),
                                                     out.ctypes.data_as(C.POINTER(C.c_double)), _stream(stream)),
                    "sph_gravity_direct_f64")
         return out
@@ -197,7 +203,7 @@ class Compute:
         """(poles [n, 24], locals [n, 16]) of the last gravity pass, by data pointer."""
         poles = np.zeros((n_nodes, 24), np.float32)
         locs = np.zeros((n_nodes, 16), np.float32)
-        _lib.check(self._lib.sph_get_tree_nodes(self._h, _ptr(poles, _fp), _ptr(locs, _fp), int(n_nodes)),
+        self._check(self._lib.sph_get_tree_nodes(self._h, _ptr(poles, _fp), _ptr(locs, _fp), int(n_nodes)),
                    "sph_get_tree_nodes")
         return poles, locs
 
@@ -218,7 +224,7 @@ class Compute:
             out = np.zeros(1 << 24, np.uint32)
         else:
             out = np.zeros(n, np.float32)
-        _lib.check(self._lib.sph_download(self._h, _lib.FIELDS[field], out.ctypes.data_as(C.c_void_p), out.size),
+        self._check(self._lib.sph_download(self._h, _lib.FIELDS[field], out.ctypes.data_as(C.c_void_p), out.size),
                    f"sph_download({field})")
         return out
 
@@ -231,7 +237,7 @@ class Compute:
             a = np.ascontiguousarray(np.asarray(values, np.uint8).reshape(-1))
         else:
             a = np.ascontiguousarray(np.asarray(values, np.float32).reshape(-1))
-        _lib.check(self._lib.sph_upload(self._h, _lib.FIELDS[field], a.ctypes.data_as(C.c_void_p), a.size),
+        self._check(self._lib.sph_upload(self._h, _lib.FIELDS[field], a.ctypes.data_as(C.c_void_p), a.size),
                    f"sph_upload({field})")
 
     def upload_async(self, field: str, values: np.ndarray, stream=None) -> None:
@@ -239,7 +245,7 @@ class Compute:
         overlap); the array must stay alive until the stream reaches the copy."""
         if not values.flags.c_contiguous:
             raise ValueError("upload_async needs a C-contiguous array")
-        _lib.check(self._lib.sph_upload_async(self._h, _lib.FIELDS[field], values.ctypes.data_as(C.c_void_p),
+        self._check(self._lib.sph_upload_async(self._h, _lib.FIELDS[field], values.ctypes.data_as(C.c_void_p),
                                               values.size, _stream(stream)), f"sph_upload_async({field})")
 
     def download_async(self, field: str, out: np.ndarray, stream=None) -> None:
@@ -247,13 +253,13 @@ class Compute:
         overlap); valid once the stream has been synchronised."""
         if not out.flags.c_contiguous:
             raise ValueError("download_async needs a C-contiguous array")
-        _lib.check(self._lib.sph_download_async(self._h, _lib.FIELDS[field], out.ctypes.data_as(C.c_void_p),
+        self._check(self._lib.sph_download_async(self._h, _lib.FIELDS[field], out.ctypes.data_as(C.c_void_p),
                                                 out.size, _stream(stream)), f"sph_download_async({field})")
 
     def device_buffer(self, field: str):
         """(device pointer, bytes, stride) of a field's storage."""
         p, b, s = C.c_void_p(), C.c_size_t(), C.c_size_t()
-        _lib.check(self._lib.sph_get_buffer(self._h, _lib.FIELDS[field], C.byref(p), C.byref(b), C.byref(s)),
+        self._check(self._lib.sph_get_buffer(self._h, _lib.FIELDS[field], C.byref(p), C.byref(b), C.byref(s)),
                    "sph_get_buffer")
         return p.value, b.value, s.value
 
@@ -271,11 +277,11 @@ class Compute:
 
     def health(self) -> int:
         w = C.c_uint32()
-        _lib.check(self._lib.sph_get_health(self._h, C.byref(w)), "sph_get_health")
+        self._check(self._lib.sph_get_health(self._h, C.byref(w)), "sph_get_health")
         return w.value
 
     def clear_health(self):
-        _lib.check(self._lib.sph_clear_health(self._h), "sph_clear_health")
+        self._check(self._lib.sph_clear_health(self._h), "sph_clear_health")
 
     def state(self) -> dict:
         names = ("pos", "vel", "acc", "rho", "u", "mass", "pressure", "h", "grad_term", "sound_speed", "du",

@@ -395,6 +395,42 @@ __global__ void __launch_bounds__(128) k_down(DownArgs a, int level, int64_t lev
         const float4 *lp = a.locals + (size_t)dp * kLocalQ;
         const float4 L0 = lp[0], L1 = lp[1], L2 = lp[2], L3 = lp[3];
         const float lx = L0.x, ly = L0.y, lz = L0.z;
+#ifdef SPH_PARITY
+        // Parity build: one lane walks the list in order and adds every
+        // contribution straight into the node's local expansion, which is the
+        // reference's summation order (helpers.h:34-45, 125-147).
+        float le[10] = {L0.w, L1.x, L1.y, L1.z, L1.w, L2.x, L2.y, L2.z, L2.w, L3.x};
+        if (lane == 0) {
+            for (int i = 0; i < cap; ++i) {
+                int e = in[i];
+                if (e < -1 || e > a.tree_cap - 10) {
+                    raise_health(a.health, SPH_HEALTH_LIST_CAPACITY);
+                    e = -1;
+                }
+                if (e == -1) break;
+                const float4 *bp = a.poles + (size_t)T[e + 1] * kPoleQ;
+                const float4 b0 = bp[0], b1 = bp[1], b2 = bp[2];
+                if ((np != 0 && T[e] != 0) || mac_accept(s0.w, s0.x, s0.y, s0.z, s_min_grav, b0, b1, b2)) {
+                    m2l_add(lx, ly, lz, b0, b1, b2, le);
+                    continue;
+                }
+                for (int k = 0; k < 8; ++k) {
+                    const int c = T[e + 2 + k];
+                    if (c == tp || c == -1) continue;
+                    const float4 *cp = a.poles + (size_t)T[c + 1] * kPoleQ;
+                    const float4 c0v = cp[0], c1v = cp[1], c2v = cp[2];
+                    const bool force = np != 0 || T[c] != 0 || op == cap;
+                    if (force || mac_accept(s0.w, s0.x, s0.y, s0.z, s_min_grav, c0v, c1v, c2v))
+                        m2l_add(lx, ly, lz, c0v, c1v, c2v, le);
+                    else
+                        out[op++] = c;
+                }
+            }
+            if (np == 0 && op < cap) out[op] = -1;
+        }
+#pragma unroll
+        for (int j = 0; j < 10; ++j) le[j] = __shfl_sync(0xffffffffu, le[j], 0);
+#else
         float acc[10];
 #pragma unroll
         for (int j = 0; j < 10; ++j) acc[j] = 0.f;
@@ -468,6 +504,7 @@ __global__ void __launch_bounds__(128) k_down(DownArgs a, int level, int64_t lev
         }
         float le[10] = {L0.w + acc[0], L1.x + acc[1], L1.y + acc[2], L1.z + acc[3], L1.w + acc[4],
                         L2.x + acc[5], L2.y + acc[6], L2.z + acc[7], L2.w + acc[8], L3.x + acc[9]};
+#endif
         if (np == 0) {
             // L2L.metal:56-70 to every active child (empty slots skipped)
             if (lane < 8) {

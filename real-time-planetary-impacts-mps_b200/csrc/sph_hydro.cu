@@ -5,13 +5,15 @@
 // step         SPH/Shaders/step.metal:12-46            (Compute.cpp:242-263)
 // snapshot     SPH/Shaders/render.metal:49-66          (Compute.cpp:396-448)
 //
-// One thread per particle in sorted (Morton cell) order, so a warp's threads
-// walk neighbouring cells together.  Neighbour data are read from sorted,
-// 16-byte records (sp4/sv4, then sA/sB/sC written by the density epilogue),
-// so every cell's particles are one contiguous run of float4 loads instead of
-// the reference's index-chased float3 gathers.  The neighbour loops visit
-// cells and particles in the reference's order and accumulate in the same
-// order, so sums agree with it to rounding.
+// A small group of lanes per particle in sorted (Morton cell) order (see
+// group_walk), so a warp's groups walk neighbouring cells together.
+// Neighbour data are read from sorted, 16-byte records (sp4/sv4, then
+// sA/sB/sC written by the density epilogue), so every cell's particles are
+// one contiguous run of float4 loads instead of the reference's index-chased
+// float3 gathers.  The neighbour walks visit the reference's cells and
+// particles; each lane sums its slice in the reference's order and the slices
+// are combined at the end (with one lane per particle, in the parity build,
+// the order is the reference's exactly).
 //
 // The reference's 128-entry per-thread neighbour cache (density.metal:67-70)
 // is replaced by rescanning the same cell box with the same filters: the
@@ -30,6 +32,17 @@ namespace {
 // floor(x / CELL_WIDTH); 2e-4 Mm keeps every particle of a cell inside its box.
 constexpr float kCellMargin = 2e-4f;
 
+// Lanes per particle in the density and acceleration walks.  The parity
+// build (SPH_PARITY) uses one, which sums in the reference's sequential order.
+#ifdef SPH_PARITY
+constexpr int kLanesPerParticle = 1;
+#else
+#ifndef SPH_HYDRO_LANES
+#define SPH_HYDRO_LANES 8
+#endif
+constexpr int kLanesPerParticle = SPH_HYDRO_LANES;
+#endif
+
 // Squared distance from (px, py, pz) to the box of cell (x, y, z), each axis
 // gap shortened by the margin.
 __device__ __forceinline__ float cell_gap2(float px, float py, float pz, int x, int y, int z) {
@@ -40,25 +53,6 @@ __device__ __forceinline__ float cell_gap2(float px, float py, float pz, int x, 
     return gx * gx + gy * gy + gz * gz;
 }
 
-// Visit the neighbours of (px, py, pz) in the cell box of radius 2h, in the
-// reference's order (x outer, z inner; sorted index within a cell).  Cells
-// farther than sqrt(r2cull) are skipped: when r2cull bounds the caller's own
-// distance filter, none of their particles would pass it, so the visited set
-// and its order are unchanged.
-template <class F>
-__device__ __forceinline__ void for_cells(float px, float py, float pz, float h, float r2cull,
-                                          const uint2 *__restrict__ cells, F &&body) {
-    CellBox b = cell_box(px, py, pz, h);
-    for (int x = b.lo0; x <= b.hi0; ++x)
-        for (int y = b.lo1; y <= b.hi1; ++y)
-            for (int z = b.lo2; z <= b.hi2; ++z) {
-                if (cell_gap2(px, py, pz, x, y, z) > r2cull) continue;
-                uint2 r = __ldg(cells + cell_index_of(x, y, z));
-                if (r.x == 0xffffffffu) continue;
-                for (uint32_t k = r.x; k <= r.y; ++k) body(k);
-            }
-}
-
 __global__ void k_gather(int n, const uint32_t *__restrict__ cidx, const float4 *__restrict__ pos4,
                          const float4 *__restrict__ vel4, float4 *__restrict__ sp4, float4 *__restrict__ sv4) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -66,6 +60,168 @@ __global__ void k_gather(int n, const uint32_t *__restrict__ cidx, const float4 
     uint32_t i = cidx[k];
     sp4[k] = pos4[i];
     sv4[k] = vel4[i];
+}
+
+// ---- neighbour walk shared by the lanes of one particle -------------------
+//
+// Each particle gets a group of L consecutive lanes (L = 1, 2, 4 or 8); a
+// warp holds 32 / L consecutive particles of the sorted order.  The group
+// walks the particle's own cell box of radius 2h in the reference's order
+// (x outer, z inner; sorted index within a cell): its lanes look up L cells
+// at a time (cells farther than the search radius are not looked up), the
+// particles of those cells are numbered consecutively, and lane `sub` takes
+// every L-th of them.  So each lane sees a slice of exactly the candidates the
+// reference's box walk visits, the lanes stay busy although a cell holds only
+// a few particles, and the cell table is read once per cell and particle
+// group instead of once per lane.  Partial sums are combined across the
+// group by a butterfly (every lane ends with the same bits).  With L = 1 the
+// walk is the reference's sequential order exactly.
+
+template <int L>
+__device__ __forceinline__ unsigned group_mask(int lane) {
+    return L == 32 ? 0xffffffffu : (((1u << L) - 1u) << (lane & ~(L - 1)));
+}
+template <int L>
+__device__ __forceinline__ float group_sum(float v, unsigned gm) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gm, v, o, L);
+    return v;
+}
+template <int L>
+__device__ __forceinline__ int group_sum_i(int v, unsigned gm) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gm, v, o, L);
+    return v;
+}
+template <int L>
+__device__ __forceinline__ float group_max(float v, unsigned gm) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) v = fmax_ref(v, __shfl_xor_sync(gm, v, o, L));
+    return v;
+}
+
+// s_off / s_start: this warp's 32-entry scratch in shared memory; gbase =
+// the group's first lane within the warp.
+template <int L, class Body>
+__device__ __forceinline__ void group_walk(float px, float py, float pz, float h, float r2cull,
+                                           const uint2 *__restrict__ cells, int sub, unsigned gm, int gbase,
+                                           uint32_t *s_off, uint32_t *s_start, Body &&body) {
+    const CellBox b = cell_box(px, py, pz, h);
+    const int ny = b.hi1 - b.lo1 + 1, nz = b.hi2 - b.lo2 + 1;
+    const int nyz = ny * nz;
+    const int nc = (b.hi0 - b.lo0 + 1) * nyz;
+    for (int c0 = 0; c0 < nc; c0 += L) {
+        const int c = c0 + sub;
+        uint32_t st = 0u, cnt = 0u;
+        if (c < nc) {
+            const int ix = c / nyz, rem = c - ix * nyz;
+            const int iy = rem / nz, iz = rem - iy * nz;
+            const int x = b.lo0 + ix, y = b.lo1 + iy, z = b.lo2 + iz;
+            if (cell_gap2(px, py, pz, x, y, z) <= r2cull) {
+                const uint2 r = __ldg(cells + cell_index_of(x, y, z));
+                if (r.x != 0xffffffffu) {
+                    st = r.x;
+                    cnt = r.y - r.x + 1u;
+                }
+            }
+        }
+        if (L == 1) {
+            for (uint32_t k = st; k < st + cnt; ++k) body(k);
+            continue;
+        }
+        uint32_t inc = cnt;
+#pragma unroll
+        for (int o = 1; o < L; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(gm, inc, o, L);
+            if (sub >= o) inc += y;
+        }
+        const uint32_t tot = __shfl_sync(gm, inc, L - 1, L);
+        if (tot == 0u) continue;
+        s_off[gbase + sub] = inc - cnt;
+        s_start[gbase + sub] = st;
+        __syncwarp(gm);
+        for (uint32_t j = sub; j < tot; j += L) {
+            int q = 0;  // the last cell whose first candidate number is <= j
+#pragma unroll
+            for (int step = L / 2; step > 0; step >>= 1)
+                if (s_off[gbase + q + step] <= j) q += step;
+            body(s_start[gbase + q] + (j - s_off[gbase + q]));
+        }
+        __syncwarp(gm);
+    }
+}
+
+// Collect, in the walk's order, the indices of the candidates of the
+// particle's box of radius 2 hbox that pass `test` into the group's list in
+// shared memory: each round of L candidates is ordered by a ballot, so the
+// list keeps the reference's visiting order.  Whenever the list could
+// overflow, `drain(count)` consumes it and the list restarts; a drain that
+// returns false keeps the list instead and the walk only counts from then on,
+// so the return value (the number of candidates found) may exceed cap.
+template <int L, class Test, class Drain>
+__device__ __forceinline__ int group_collect(float px, float py, float pz, float hbox, float r2cull,
+                                             const uint2 *__restrict__ cells, int sub, unsigned gm, int gbase,
+                                             uint32_t *s_off, uint32_t *s_start, uint32_t *list, int cap,
+                                             Test &&test, Drain &&drain) {
+    const CellBox b = cell_box(px, py, pz, hbox);
+    const int ny = b.hi1 - b.lo1 + 1, nz = b.hi2 - b.lo2 + 1;
+    const int nyz = ny * nz;
+    const int nc = (b.hi0 - b.lo0 + 1) * nyz;
+    int cnt = 0;
+    for (int c0 = 0; c0 < nc; c0 += L) {
+        const int c = c0 + sub;
+        uint32_t st = 0u, n_in = 0u;
+        if (c < nc) {
+            const int ix = c / nyz, rem = c - ix * nyz;
+            const int iy = rem / nz, iz = rem - iy * nz;
+            const int x = b.lo0 + ix, y = b.lo1 + iy, z = b.lo2 + iz;
+            if (cell_gap2(px, py, pz, x, y, z) <= r2cull) {
+                const uint2 r = __ldg(cells + cell_index_of(x, y, z));
+                if (r.x != 0xffffffffu) {
+                    st = r.x;
+                    n_in = r.y - r.x + 1u;
+                }
+            }
+        }
+        uint32_t inc = n_in;
+#pragma unroll
+        for (int o = 1; o < L; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(gm, inc, o, L);
+            if (sub >= o) inc += y;
+        }
+        const uint32_t tot = __shfl_sync(gm, inc, L - 1, L);
+        if (tot == 0u) continue;
+        s_off[gbase + sub] = inc - n_in;
+        s_start[gbase + sub] = st;
+        __syncwarp(gm);
+        for (uint32_t j0 = 0; j0 < tot; j0 += L) {
+            const uint32_t j = j0 + sub;
+            uint32_t k = 0u;
+            bool hit = false;
+            if (j < tot) {
+                int q = 0;  // the last cell whose first candidate number is <= j
+#pragma unroll
+                for (int step = L / 2; step > 0; step >>= 1)
+                    if (s_off[gbase + q + step] <= j) q += step;
+                k = s_start[gbase + q] + (j - s_off[gbase + q]);
+                hit = test(k);
+            }
+            const unsigned hm = (__ballot_sync(gm, hit) >> gbase) & (L == 32 ? 0xffffffffu : ((1u << L) - 1u));
+            const int nh = __popc(hm);
+            if (cnt + nh > cap) {
+                if (!drain(cnt)) {
+                    cnt += nh;  // overflow: keep counting, store nothing more
+                    continue;
+                }
+                cnt = 0;
+            }
+            if (hit) list[cnt + __popc(hm & ((1u << sub) - 1u))] = k;
+            cnt += nh;
+            __syncwarp(gm);
+        }
+        __syncwarp(gm);
+    }
+    return cnt;
 }
 
 struct DensityArgs {
@@ -83,15 +239,40 @@ struct DensityArgs {
     EosTables eos;
 };
 
-__global__ void __launch_bounds__(128) k_density(DensityArgs a) {
-    const int index = blockIdx.x * blockDim.x + threadIdx.x;
-    if (index >= a.n) return;
-    if (index == 0) a.globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
+// Per-particle neighbour list of the density pass, in shared memory: the
+// sorted indices of every candidate within kListReach x the smoothing length
+// the list was built for, in the reference's visiting order.  The iteration's
+// sweeps and the gradient sweep read it instead of walking the cells again
+// (recomputing each distance exactly as the walk does); a sweep whose radius
+// the list does not cover rebuilds it, and a particle whose list overflows
+// walks the cells in every sweep.
+constexpr int kListMax = 192;       // list entries per particle
+// particles per block: 16 groups, but never fewer than a warp's worth of lanes
+template <int L>
+__host__ __device__ constexpr int parts_per_block() { return 16 * L >= 32 ? 16 : 32 / L; }
+constexpr float kListReach = 1.15f; // list radius / (2 h)
+
+// density.metal:12-239 for one sorted particle per lane group.  The group
+// keeps the reference's per-particle iteration state (h, the int max_h, the
+// cached scan's h and neighbour count) identically in all its lanes.
+template <int L>
+__global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArgs a) {
+    extern __shared__ uint32_t s_lists[];
+    __shared__ uint32_t s_off[parts_per_block<L>() * L], s_start[parts_per_block<L>() * L];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, sub = lane & (L - 1), gbase = lane & ~(L - 1);
+    uint32_t *w_off = s_off + (threadIdx.x & ~31), *w_start = s_start + (threadIdx.x & ~31);
+    uint32_t *list = s_lists + (size_t)(threadIdx.x / L) * kListMax;
+    const unsigned gm = group_mask<L>(lane);
+    const int index = t / L;
+    if (index >= a.n) return;  // whole groups leave together
+    if (t == 0) a.globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
     const uint32_t ind = a.cidx[index];
     const float4 me = a.sp4[index];
     const float4 mv = a.sv4[index];
     if (!a.active[ind]) {
         // density.metal:40-55: EOS only
+        if (sub != 0) return;
         float2 pc = eos_lookup(a.eos, a.mat[ind], a.rho[ind], a.u[ind]);
         a.P[ind] = pc.x;
         a.c[ind] = pc.y;
@@ -116,33 +297,58 @@ __global__ void __launch_bounds__(128) k_density(DensityArgs a) {
     float hs = hi, hs2x4 = h2x4;
     const uint2 *cells = a.cells;
     const float4 *sp4 = a.sp4;
+    // the list: entries within sqrt(list_r2); n_list < 0 = none
+    int n_list = -1;
+    float list_r2 = 0.f;
+    auto build = [&](float hb) {
+        const float rl = 2.f * hb * kListReach;
+        list_r2 = rl * rl;
+        const float r2max = list_r2;
+        n_list = group_collect<L>(
+            px, py, pz, hb * kListReach, r2max, cells, sub, gm, gbase, w_off, w_start, list, kListMax,
+            [&](uint32_t k) {
+                const float4 q = __ldg(sp4 + k);
+                const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                return dx * dx + dy * dy + dz * dz <= r2max;
+            },
+            [](int) { return false; });
+        __syncwarp(gm);
+    };
     while (eps > kDensityEta && count < kMaxNR) {
-        dens = 0.f;
-        if (hi < (float)max_h && nn < kNeighbourCache) {
-            const float h2 = hi + hi;
-            for_cells(px, py, pz, hs, hs2x4, cells, [&](uint32_t k) {
-                float4 q = __ldg(sp4 + k);
-                float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
-                float r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 > hs2x4) return;
-                float r = sqrtf(r2);
-                if (r > h2) return;
-                dens += kernel_w(r, h1) * q.w;
-            });
-        } else {
+        const bool cached = hi < (float)max_h && nn < kNeighbourCache;
+        if (!cached) {
             hs = hi;
             hs2x4 = h2x4;
-            nn = 0;
-            for_cells(px, py, pz, hi, h2x4, cells, [&](uint32_t k) {
-                float4 q = __ldg(sp4 + k);
-                float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
-                float r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 > h2x4) return;
-                float r = sqrtf(r2);
-                if (nn < kNeighbourCache) nn++;
-                dens += kernel_w(r, h1) * q.w;
+        }
+        const float h2 = hi + hi;
+        if (n_list < 0 || (n_list <= kListMax && hs2x4 > list_r2)) build(hs);
+        float part = 0.f;
+        int found = 0;
+        if (n_list <= kListMax) {
+            for (int i = sub; i < n_list; i += L) {
+                const float4 q = __ldg(sp4 + list[i]);
+                const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > hs2x4) continue;
+                const float r = sqrtf(r2);
+                if (cached && r > h2) continue;
+                ++found;
+                part += kernel_w(r, h1) * q.w;
+            }
+        } else {
+            group_walk<L>(px, py, pz, hs, hs2x4, cells, sub, gm, gbase, w_off, w_start, [&](uint32_t k) {
+                const float4 q = __ldg(sp4 + k);
+                const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > hs2x4) return;
+                const float r = sqrtf(r2);
+                if (cached && r > h2) return;
+                ++found;
+                part += kernel_w(r, h1) * q.w;
             });
         }
+        dens = group_sum<L>(part, gm);
+        if (!cached) nn = min(group_sum_i<L>(found, gm), kNeighbourCache);
         float nh = fmin_ref(kResolutionEta * powf(mi / dens, 1.f / 3), kMaxH);
         nh = 0.5f * (hi + nh);
         eps = fabsf(nh - hi) / hi;
@@ -154,48 +360,61 @@ __global__ void __launch_bounds__(128) k_density(DensityArgs a) {
             count++;
         }
     }
-    // gradient sweep (density.metal:145-213)
-    float dens_h = 0.f, vdiv = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+    // gradient sweep (density.metal:145-213): below N_NEIGHBOURS_ESTIM the
+    // cached neighbours (last full scan) within 2h; above, a full scan at h
+    // that adds to the converged density again
+    const bool gcached = nn < kNeighbourCache;
+    const float gh = gcached ? hs : hi;
+    const float g2 = gcached ? hs2x4 : h2x4;
+    const float h2 = hi + hi;
     const float vix = mv.x, viy = mv.y, viz = mv.z;
     const float4 *sv4 = a.sv4;
-    auto grad = [&](uint32_t k, const float4 &q, float r, float dx, float dy, float dz) {
-        float mj = q.w;
+    float pdens = 0.f, dens_h = 0.f, vdiv = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+    auto grad = [&](uint32_t k, float r, float mj, float dx, float dy, float dz) {
+        if (!gcached) pdens += kernel_w(r, h1) * mj;
         dens_h += mj * kernel_dwdh(r, h1);
         if (r > 1e-12f) {
-            float r1 = 1.f / r;
-            float4 vj = __ldg(sv4 + k);
-            float vx = vj.x - vix, vy = vj.y - viy, vz = vj.z - viz;
-            float s = kernel_gradw_scale(r, h1);
-            float gx = s * (dx * r1), gy = s * (dy * r1), gz = s * (dz * r1);
+            const float r1 = 1.f / r;
+            const float4 vj = __ldg(sv4 + k);
+            const float vx = vj.x - vix, vy = vj.y - viy, vz = vj.z - viz;
+            const float sc = kernel_gradw_scale(r, h1);
+            const float gx = sc * (dx * r1), gy = sc * (dy * r1), gz = sc * (dz * r1);
             vdiv += mj * (vx * gx + vy * gy + vz * gz);
             cx += mj * (vy * gz - vz * gy);
             cy += mj * (vz * gx - vx * gz);
             cz += mj * (vx * gy - vy * gx);
         }
     };
-    if (nn < kNeighbourCache) {
-        const float h2 = hi + hi;
-        for_cells(px, py, pz, hs, hs2x4, cells, [&](uint32_t k) {
-            float4 q = __ldg(sp4 + k);
-            float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
-            float r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 > hs2x4) return;
-            float r = sqrtf(r2);
-            if (r > h2) return;
-            grad(k, q, r, dx, dy, dz);
-        });
+    if (n_list <= kListMax && g2 > list_r2) build(gh);
+    if (n_list <= kListMax) {
+        for (int i = sub; i < n_list; i += L) {
+            const uint32_t k = list[i];
+            const float4 q = __ldg(sp4 + k);
+            const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > g2) continue;
+            const float r = sqrtf(r2);
+            if (gcached && r > h2) continue;
+            grad(k, r, q.w, dx, dy, dz);
+        }
     } else {
-        // cache overflow: the reference adds to the converged density again
-        for_cells(px, py, pz, hi, h2x4, cells, [&](uint32_t k) {
-            float4 q = __ldg(sp4 + k);
-            float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
-            float r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 > h2x4) return;
-            float r = sqrtf(r2);
-            dens += kernel_w(r, h1) * q.w;
-            grad(k, q, r, dx, dy, dz);
+        group_walk<L>(px, py, pz, gh, g2, cells, sub, gm, gbase, w_off, w_start, [&](uint32_t k) {
+            const float4 q = __ldg(sp4 + k);
+            const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > g2) return;
+            const float r = sqrtf(r2);
+            if (gcached && r > h2) return;
+            grad(k, r, q.w, dx, dy, dz);
         });
     }
+    if (!gcached) dens += group_sum<L>(pdens, gm);
+    dens_h = group_sum<L>(dens_h, gm);
+    vdiv = group_sum<L>(vdiv, gm);
+    cx = group_sum<L>(cx, gm);
+    cy = group_sum<L>(cy, gm);
+    cz = group_sum<L>(cz, gm);
+    if (sub != 0) return;
     vdiv = fabsf(vdiv) / dens;
     float acurl = sqrtf(cx * cx + cy * cy + cz * cz) / dens;
     float fi = 1.f / (1.f + (hi / (3.f * dens)) * dens_h);
@@ -225,8 +444,23 @@ struct AccelArgs {
     int32_t *globals;
 };
 
-__global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
-    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+// accelerations.metal:12-141 for one sorted particle per lane group.  The
+// walk covers the particle's own box of radius 2 min(h, MAX_SMOOTHING_LENGTH)
+// (the reference's box, which also decides which pairs with r < 2 h_j are
+// seen, Q8).  The pairs that pass the reference's test are first collected in
+// order into the group's list, then evaluated by all lanes of the group
+// together, so the long pair computation runs with every lane busy.
+template <int L>
+__global__ void __launch_bounds__(parts_per_block<L>() * L) k_acceleration(AccelArgs a) {
+    extern __shared__ uint32_t s_lists[];
+    __shared__ uint32_t s_off[parts_per_block<L>() * L], s_start[parts_per_block<L>() * L];
+    __shared__ int wmin[32];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, sub = lane & (L - 1), gbase = lane & ~(L - 1);
+    uint32_t *w_off = s_off + (threadIdx.x & ~31), *w_start = s_start + (threadIdx.x & ~31);
+    uint32_t *list = s_lists + (size_t)(threadIdx.x / L) * kListMax;
+    const unsigned gm = group_mask<L>(lane);
+    const int index = t / L;
     int idt = 0x7fffffff;
     if (index < a.n) {
         const uint32_t ind = a.cidx[index];
@@ -240,13 +474,11 @@ __global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
             float dvx = 0.f, dvy = 0.f, dvz = 0.f, du = 0.f, dh = 0.f;
             float vsig_i = 1e-12f;
             const float4 *sA = a.sA, *sB = a.sB, *sC = a.sC;
-            for_cells(xi, yi, zi, fmin_ref(hi, kMaxH), 3.402823466e+38f, a.cells, [&](uint32_t k) {
+            auto pair = [&](uint32_t k) {
                 const float4 Aj = __ldg(sA + k);
                 const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
                 const float r2 = dx * dx + dy * dy + dz * dz;
                 const float hj = Aj.w;
-                const float hj2x4 = hj * hj * 4.f;
-                if ((r2 > hi2x4 && r2 > hj2x4) || r2 < 1e-12f) return;
                 const float4 Cj = __ldg(sC + k);
                 const float4 Bj = __ldg(sB + k);
                 const float r = sqrtf(r2);
@@ -271,14 +503,31 @@ __global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
                 dvz -= mj * (facti * giz + factj * gjz + nu * gz);
                 du += mj * (facti * (vx * gix + vy * giy + vz * giz) + 0.5f * nu * (vx * gx + vy * gy + vz * gz));
                 dh += (mj / rhoj) * (vx * gix + vy * giy + vz * giz);
-            });
-            float4 acc = a.acc4[ind];
-            acc.x += dvx;
-            acc.y += dvy;
-            acc.z += dvz;
-            a.acc4[ind] = acc;
-            a.du[ind] = du;
-            a.dhdt[ind] = dh;
+            };
+            auto drain = [&](int cnt) {
+                __syncwarp(gm);
+                for (int i = sub; i < cnt; i += L) pair(list[i]);
+                __syncwarp(gm);
+                return true;
+            };
+            const int rest = group_collect<L>(
+                xi, yi, zi, fmin_ref(hi, kMaxH), 3.402823466e+38f, a.cells, sub, gm, gbase, w_off, w_start, list,
+                kListMax,
+                [&](uint32_t k) {
+                    const float4 Aj = __ldg(sA + k);
+                    const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    const float hj2x4 = Aj.w * Aj.w * 4.f;
+                    return !((r2 > hi2x4 && r2 > hj2x4) || r2 < 1e-12f);
+                },
+                drain);
+            drain(rest);
+            dvx = group_sum<L>(dvx, gm);
+            dvy = group_sum<L>(dvy, gm);
+            dvz = group_sum<L>(dvz, gm);
+            du = group_sum<L>(du, gm);
+            dh = group_sum<L>(dh, gm);
+            vsig_i = group_max<L>(vsig_i, gm);
             // accelerations.metal:129-140
             const float goal = 2.0f * kCFL * kGamma * hi / vsig_i;
             int r = 0;
@@ -288,16 +537,24 @@ __global__ void __launch_bounds__(128) k_acceleration(AccelArgs a) {
                 r++;
             }
             idt = (int)ceilf(1 / kDtMin1 * cand);
-            a.nat[ind] = a.globals[0] + idt;
+            if (sub == 0) {
+                float4 acc = a.acc4[ind];
+                acc.x += dvx;
+                acc.y += dvy;
+                acc.z += dvz;
+                a.acc4[ind] = acc;
+                a.du[ind] = du;
+                a.dhdt[ind] = dh;
+                a.nat[ind] = a.globals[0] + idt;
+            }
         }
     }
     // block-wide minimum, then one atomic per block
     for (int o = 16; o > 0; o >>= 1) idt = min(idt, __shfl_xor_sync(0xffffffffu, idt, o));
-    __shared__ int wmin[32];
-    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = idt;
+    if (lane == 0) wmin[threadIdx.x >> 5] = idt;
     __syncthreads();
     if (threadIdx.x < 32) {
-        int v = (threadIdx.x < (blockDim.x >> 5)) ? wmin[threadIdx.x] : 0x7fffffff;
+        int v = (threadIdx.x < ((blockDim.x + 31) >> 5)) ? wmin[threadIdx.x] : 0x7fffffff;
         for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
         if (threadIdx.x == 0 && v != 0x7fffffff) atomicMin(&a.globals[1], v);
     }
@@ -357,6 +614,22 @@ __global__ void k_snapshot(int n, const float4 *__restrict__ pos4, const int32_t
     atomicMax(img + pixel, mat[i]);
 }
 
+// Dynamic shared memory of the list kernels; above 48 KiB (the one-lane
+// parity build) it needs the per-device opt-in, set once per device.
+size_t list_smem_opt_in() {
+    const size_t smem = sizeof(uint32_t) * parts_per_block<kLanesPerParticle>() * kListMax;
+    static bool done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (smem > 48 * 1024 && dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(k_density<kLanesPerParticle>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_acceleration<kLanesPerParticle>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        done[dev] = true;
+    }
+    return smem;
+}
+
 }  // namespace
 
 sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
@@ -385,7 +658,9 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     a.globals = ctx->globals;
     a.health = ctx->health;
     a.eos = ctx->eos;
-    k_density<<<(n + 127) / 128, 128, 0, st>>>(a);
+    constexpr int parts = parts_per_block<kLanesPerParticle>();
+    const size_t smem = list_smem_opt_in();
+    k_density<kLanesPerParticle><<<(unsigned)((n + parts - 1) / parts), parts * kLanesPerParticle, smem, st>>>(a);
     return cuda_status(cudaGetLastError(), "density");
 }
 
@@ -405,7 +680,9 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     a.nat = ctx->nat;
     a.active = ctx->active;
     a.globals = ctx->globals;
-    k_acceleration<<<(n + 127) / 128, 128, 0, st>>>(a);
+    constexpr int parts = parts_per_block<kLanesPerParticle>();
+    const size_t smem = list_smem_opt_in();
+    k_acceleration<kLanesPerParticle><<<(unsigned)((n + parts - 1) / parts), parts * kLanesPerParticle, smem, st>>>(a);
     return cuda_status(cudaGetLastError(), "acceleration");
 }
 

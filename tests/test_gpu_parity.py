@@ -36,6 +36,11 @@ INT_FIELDS = {"cell_key", "cell_index", "active", "next_active_time", "dt", "glo
 TOL = {"acc": 3e-3, "grav_norm": 3e-3, "h": 1e-5, "rho": 1e-5, "grad_term": 1e-5, "pressure": 1e-4,
        "sound_speed": 1e-4, "balsara": 1e-4, "du": 1e-4, "dhdt": 1e-4, "pos": 1e-6, "vel": 3e-3, "u": 1e-5}
 P99_TOL = {"acc": 1e-3, "grav_norm": 1e-3, "vel": 1e-4}
+# The product build sums each particle's neighbours in 8 interleaved slices
+# (one per lane of its group) and adds the slices at the end, so its float sums
+# differ from the reference's sequential ones by rounding: ~5e-7 relative on
+# density, which the steep EOS table turns into up to ~1e-4 on pressure.
+TOL_PRODUCT = dict(TOL, pressure=5e-4, sound_speed=5e-4, balsara=1e-3, du=1e-3, dhdt=1e-3)
 PASS_METHOD = {"sort": "sort", "gravity": "gravitationalPass", "density": "densityPass",
                "acceleration": "accelerationPass", "step": "stepPass"}
 
@@ -54,7 +59,8 @@ def rel_err(a, b):
     return d / np.maximum(m, floor)
 
 
-def compare(field, got, want, where):
+def compare(field, got, want, where, tol=None):
+    tol = TOL if tol is None else tol
     if field in INT_FIELDS:
         bad = np.nonzero(np.asarray(got).reshape(-1) != np.asarray(want).reshape(-1))[0]
         assert bad.size == 0, f"{where} {field}: {bad.size} mismatches, first at {bad[:5]}"
@@ -63,7 +69,7 @@ def compare(field, got, want, where):
     worst = float(e.max()) if e.size else 0.0
     print(f"  {where:28s} {field:12s} max rel err {worst:.3e}  p99 {np.percentile(e, 99):.3e}")
     assert np.all(np.isfinite(np.asarray(got))), f"{where} {field}: non-finite values"
-    assert worst <= TOL[field], f"{where} {field}: max rel err {worst:.3e} > {TOL[field]:.1e}"
+    assert worst <= tol[field], f"{where} {field}: max rel err {worst:.3e} > {tol[field]:.1e}"
     if field in P99_TOL and e.size:
         p99 = float(np.percentile(e, 99))
         assert p99 <= P99_TOL[field], f"{where} {field}: p99 rel err {p99:.3e} > {P99_TOL[field]:.1e}"
@@ -106,13 +112,18 @@ def test_sort_and_cells_bit_exact(cuda, pkg, O, eos_grids):
         assert np.array_equal(c.download("cell_end"), st.cell_end)
 
 
-def test_every_pass_matches_reference_two_steps(cuda, pkg):
+@pytest.mark.parametrize("build", ["parity", "product"])
+def test_every_pass_matches_reference_two_steps(cuda, pkg, build):
     """Each pass against the reference's own outputs (golden), with the
     reference's CPU octree; each step starts from the reference's state."""
     g = golden("steps_impact_2560.npz")
     ic = {k[3:]: v for k, v in g.items() if k.startswith("ic_")}
     print()
-    with pkg.Compute(ic, tree_source="host", max_children_in_leaf=8) as c:
+    parity = build == "parity"
+    if parity:
+        pkg.build(parity=True)
+    tol = TOL if parity else TOL_PRODUCT
+    with pkg.Compute(ic, tree_source="host", max_children_in_leaf=8, parity=parity) as c:
         for s in range(2):
             if s == 1:
                 # restart from the reference's state after step 0
@@ -129,7 +140,7 @@ def test_every_pass_matches_reference_two_steps(cuda, pkg):
                 getattr(c, PASS_METHOD[p])()
                 c.synchronize()
                 for f in fields:
-                    compare(f, c.download(f), g[f"s{s}_{p}_{f}"], f"step {s} {p}")
+                    compare(f, c.download(f), g[f"s{s}_{p}_{f}"], f"{build} step {s} {p}", tol)
 
 
 def test_gpu_tree_matches_oracle_morton_tree(cuda, pkg, O):
