@@ -173,6 +173,7 @@ static void tree_storage_free(Tree &t) {
     cudaFree(t.lists[0]);
     cudaFree(t.lists[1]);
     cudaFree(t.meta);
+    cudaFree(t.node_range);
     Tree fresh;
     fresh.list_cap = t.list_cap;
     t = fresh;
@@ -199,6 +200,7 @@ static sph_status tree_storage_alloc(Tree &t, int64_t node_cap, int64_t tree_cap
     if (e == cudaSuccess) e = dmalloc(&t.lists[0], (size_t)branch_cap * list_cap + 2);
     if (e == cudaSuccess) e = dmalloc(&t.lists[1], (size_t)branch_cap * list_cap + 2);
     if (e == cudaSuccess) e = dmalloc(&t.meta, 4);
+    if (e == cudaSuccess) e = dmalloc(&t.node_range, node_cap);
     if (e == cudaSuccess) e = cudaMemset(t.level_count, 0, sizeof(int32_t) * 16);
     if (e == cudaSuccess) e = cudaMemset(t.parent_slot, 0, sizeof(int32_t) * node_cap);
     return cuda_status(e, "tree storage");

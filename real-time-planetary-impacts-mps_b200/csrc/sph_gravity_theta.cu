@@ -4,24 +4,26 @@
 // acceptance test without an opening angle, force-accepts failing leaves and
 // keeps integer-truncated softening coefficients (kernels.h:93,97).
 //
-// Tree and passes keep the reference's structure (flattened int tree, one
-// launch per level, lists inherited from the parent), with these changes:
-//   * multipoles: mass, centre of mass, the full second moments
-//     Q_jk = sum m r_j r_k about the centre of mass, and the radius of the
-//     smallest sphere about the centre of mass that holds the node's box;
-//   * acceptance: (r_A + r_B) < theta * |com_A - com_B|, and never closer than
-//     the softening support 2 eps (so every softened pair is summed exactly);
-//   * branch targets: accepted nodes go through M2L into a local expansion of
-//     the potential, the acceleration (monopole + quadrupole) and its gradient
-//     (monopole); a rejected node is passed to the target's list, or opened
-//     one level first when it is larger than the target;
-//   * leaf targets resolve their list completely: accepted nodes are
-//     evaluated at each particle (M2P, monopole + quadrupole), rejected
-//     leaves are summed particle by particle (P2P, the cubic-spline softened
-//     kernel with its exact coefficients), rejected branches are opened
-//     through a small per-warp stack.  Per-particle sums are Kahan-compensated.
-// Locals hold no factor G, like the reference's; the leaf writes
-// acc = G a, |a| (the reference's gravNorm) and the potential G phi.
+// Tree: the GPU Morton octree (sph_tree.cu), whose leaves hold contiguous
+// runs of the particles in key order.  Up pass, one launch per level: per
+// node the mass, centre of mass, the second moments Q_jk = sum m r_j r_k about
+// the centre of mass, and the radius of the smallest sphere about the centre
+// of mass that holds the node's box.
+//
+// Evaluation is a group walk: a warp takes 32 consecutive particles in key
+// order (a compact group) and traverses the tree from the root, 32 nodes at a
+// time from a queue.  A node is accepted for the whole group when
+//     r_node < theta * d   and   d > 2 eps,
+// d being the distance from its centre of mass to the group's bounding box
+// (so every particle of the group sees it under an angle below theta and
+// outside the softening support); accepted nodes are evaluated at each
+// particle (M2P: monopole + quadrupole, potential and acceleration), rejected
+// leaves are summed particle by particle (P2P with the cubic-spline softened
+// kernel and its exact coefficients), rejected branches put their children on
+// the queue.  Accepted nodes and rejected leaves are staged in shared memory
+// and evaluated in batches with every lane busy; each batch's partial sums
+// are added into Kahan-compensated per-particle accumulators.  The walk
+// writes acc = G a, |a| (the reference's gravNorm) and the potential G phi.
 #include <cuda_runtime.h>
 
 #include "sph_internal.h"
@@ -33,10 +35,6 @@ namespace {
 // Layout of a theta-form node record (kPoleQ float4 per node):
 //   q0 (com.xyz, radius)  q1 (M, Qxx, Qxy, Qxz)  q2 (Qyy, Qyz, Qzz, 0)
 //   q3 (bbox min, 0)      q4 (bbox max, 1)
-// and of a local (kLocalQ float4): l0 (centre.xyz, phi0)  l1 (ax, ay, az, Txx)
-//   l2 (Txy, Txz, Tyy, Tyz)  l3 (Tzz, 0, 0, 0)   with T_ij = d a_i / d x_j.
-
-constexpr int kStack = 128;  // per-warp stack of opened branches at a leaf
 
 __device__ __forceinline__ float corner_radius(float cx, float cy, float cz, float mnx, float mny, float mnz,
                                                float mxx, float mxy, float mxz) {
@@ -168,38 +166,6 @@ __global__ void k_up_theta(ThetaUpArgs a, int level, int64_t level_cap) {
     }
 }
 
-// Field of a node (mass M, second moments Q about its centre of mass) at
-// R = x - com: potential (without the factor -G... see below), acceleration
-// and, for M2L, the monopole gradient.  With D = 1/|R|:
-//   phi  = -(M D + 1/2 Q_jk d_j d_k D)
-//   a_i  =   M d_i D + 1/2 Q_jk d_i d_j d_k D
-//   T_ij =   M d_i d_j D
-struct Field {
-    float phi, ax, ay, az;
-};
-
-__device__ __forceinline__ Field node_field(float Rx, float Ry, float Rz, const float4 &q1, const float4 &q2) {
-    const float r2 = Rx * Rx + Ry * Ry + Rz * Rz;
-    const float rinv = 1.f / sqrtf(r2);
-    const float rinv2 = rinv * rinv;
-    const float rinv3 = rinv * rinv2;
-    const float rinv5 = rinv3 * rinv2;
-    const float rinv7 = rinv5 * rinv2;
-    const float M = q1.x, Qxx = q1.y, Qxy = q1.z, Qxz = q1.w, Qyy = q2.x, Qyz = q2.y, Qzz = q2.z;
-    const float QRx = Qxx * Rx + Qxy * Ry + Qxz * Rz;
-    const float QRy = Qxy * Rx + Qyy * Ry + Qyz * Rz;
-    const float QRz = Qxz * Rx + Qyz * Ry + Qzz * Rz;
-    const float RQR = Rx * QRx + Ry * QRy + Rz * QRz;
-    const float trQ = Qxx + Qyy + Qzz;
-    Field f;
-    f.phi = -(M * rinv + 0.5f * (3.f * RQR * rinv5 - trQ * rinv3));
-    const float radial = -M * rinv3 - 7.5f * RQR * rinv7 + 1.5f * trQ * rinv5;
-    f.ax = radial * Rx + 3.f * QRx * rinv5;
-    f.ay = radial * Ry + 3.f * QRy * rinv5;
-    f.az = radial * Rz + 3.f * QRz * rinv5;
-    return f;
-}
-
 // Cubic-spline softened pair kernel with its exact coefficients (the
 // reference's kernels.h:87-102 truncates them): force factor f(r) with
 // a = -m f(r) R / r, and potential phi(r) (both -> Newtonian for r >= 2 eps).
@@ -224,6 +190,23 @@ __device__ __forceinline__ void soft_pair(float r, float &fr, float &pot) {
     }
 }
 
+__device__ __forceinline__ float warp_reduce_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_reduce_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float warp_reduce_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
     const float y = v - c;
     const float t = s + y;
@@ -231,307 +214,285 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
     s = t;
 }
 
-struct ThetaDownArgs {
+// ---- the group walk ----------------------------------------------------------
+constexpr int kWalkWarps = 4;    // warps per block
+constexpr int kCellCap = 64;     // accepted nodes staged per warp before evaluation
+constexpr int kLeafCap = 64;     // rejected leaves staged per warp before evaluation
+constexpr int kStackInts = 8192; // per warp, in global memory (depth-first: <= depth x 256 in use)
+
+__global__ void k_gather_key_order(int n, const uint32_t *__restrict__ order, const float4 *__restrict__ pos4,
+                                   float4 *__restrict__ kp4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) kp4[i] = pos4[order[i]];
+}
+
+struct WalkArgs {
     const int32_t *T;
-    const int32_t *level_nodes;
-    const int32_t *level_count;
-    const int32_t *list_slot;
-    const int32_t *parent_slot;
     const float4 *poles;
-    float4 *locals;
-    const int32_t *list_in;
-    int32_t *list_out;
-    int list_cap;
-    int64_t branch_cap;
-    int64_t tree_cap;
-    float theta;
-    const float4 *pos4;
+    const int2 *node_range;
+    const float4 *kp4;        // positions and masses in key order
+    const uint32_t *order;    // key order -> particle id
+    int n, ngroups;
+    float theta2;
     float4 *acc4;
-    float *gnorm;
-    float *phi;
+    float *gnorm, *phi;
+    int32_t *queues;
+    uint32_t *counter;
     uint32_t *health;
 };
 
-__device__ __forceinline__ bool accept_theta(float ax, float ay, float az, float ra, const float4 &b0, float theta) {
-    const float dx = ax - b0.x, dy = ay - b0.y, dz = az - b0.z;
-    const float d2 = dx * dx + dy * dy + dz * dz;
-    const float rs = ra + b0.w;
-    const float dmin = 2.f * kGravSoft;
-    return rs * rs < theta * theta * d2 && d2 > dmin * dmin;
+// Acceleration (and potential) of the staged nodes at x, per unit G.
+__device__ __forceinline__ void eval_cells(const float4 (*cell)[3], int ncell, float4 x, float &sx, float &sy, float &sz,
+                                           float &sp) {
+    for (int j = 0; j < ncell; ++j) {
+        const float4 c0 = cell[j][0], c1 = cell[j][1], c2 = cell[j][2];
+        // c0 = (com, M), c1 = (Qxx, Qxy, Qxz, Qyy), c2 = (Qyz, Qzz, -, -)
+        const float Rx = x.x - c0.x, Ry = x.y - c0.y, Rz = x.z - c0.z;
+        const float r2 = Rx * Rx + Ry * Ry + Rz * Rz;
+        const float rinv = rsqrtf(r2);
+        const float rinv2 = rinv * rinv;
+        const float rinv3 = rinv * rinv2;
+        const float rinv5 = rinv3 * rinv2;
+        const float M = c0.w, Qxx = c1.x, Qxy = c1.y, Qxz = c1.z, Qyy = c1.w, Qyz = c2.x, Qzz = c2.y;
+        const float QRx = Qxx * Rx + Qxy * Ry + Qxz * Rz;
+        const float QRy = Qxy * Rx + Qyy * Ry + Qyz * Rz;
+        const float QRz = Qxz * Rx + Qyz * Ry + Qzz * Rz;
+        const float RQR = Rx * QRx + Ry * QRy + Rz * QRz;
+        const float trQ = Qxx + Qyy + Qzz;
+        const float q5 = RQR * rinv5;
+        sp -= M * rinv + 0.5f * (3.f * q5 - trQ * rinv3);
+        const float radial = -M * rinv3 - 7.5f * q5 * rinv2 + 1.5f * trQ * rinv5;
+        const float t3 = 3.f * rinv5;
+        sx += radial * Rx + t3 * QRx;
+        sy += radial * Ry + t3 * QRy;
+        sz += radial * Rz + t3 * QRz;
+    }
 }
 
-// M2L of node b into the local accumulators at centre (lx, ly, lz).
-__device__ __forceinline__ void m2l_theta(float lx, float ly, float lz, const float4 *bp, float *acc) {
-    const float4 b0 = bp[0], b1 = bp[1], b2 = bp[2];
-    const float Rx = lx - b0.x, Ry = ly - b0.y, Rz = lz - b0.z;
-    const Field f = node_field(Rx, Ry, Rz, b1, b2);
-    const float r2 = Rx * Rx + Ry * Ry + Rz * Rz;
-    const float rinv = 1.f / sqrtf(r2);
-    const float rinv3 = rinv * rinv * rinv;
-    const float m3 = 3.f * b1.x * rinv3 * rinv * rinv;
-    const float m1 = b1.x * rinv3;
-    acc[0] += f.phi;
-    acc[1] += f.ax;
-    acc[2] += f.ay;
-    acc[3] += f.az;
-    acc[4] += m3 * Rx * Rx - m1;
-    acc[5] += m3 * Rx * Ry;
-    acc[6] += m3 * Rx * Rz;
-    acc[7] += m3 * Ry * Ry - m1;
-    acc[8] += m3 * Ry * Rz;
-    acc[9] += m3 * Rz * Rz - m1;
+// Softened pair sums of the staged particles at x, per unit G.
+__device__ __forceinline__ void eval_parts(const float4 *part, int np, float4 x, float &sx, float &sy, float &sz,
+                                           float &sp) {
+    const float soft2x4 = 4.f * kGravSoft * kGravSoft;
+    for (int j = 0; j < np; ++j) {
+        const float4 q = part[j];
+        const float rx = x.x - q.x, ry = x.y - q.y, rz = x.z - q.z;
+        const float r2 = rx * rx + ry * ry + rz * rz;
+        if (r2 >= soft2x4) {
+            const float rinv = rsqrtf(r2);
+            const float mr = q.w * rinv;
+            const float s = -mr * rinv * rinv;
+            sx += s * rx;
+            sy += s * ry;
+            sz += s * rz;
+            sp -= mr;
+        } else if (r2 > 0.f) {
+            const float r = sqrtf(r2);
+            float fr, pot;
+            soft_pair(r, fr, pot);
+            const float s = -q.w * fr / r;
+            sx += s * rx;
+            sy += s * ry;
+            sz += s * rz;
+            sp += q.w * pot;
+        }
+    }
 }
 
-__device__ void branch_target(const ThetaDownArgs &a, int tp, int dp, int lane) {
+__global__ void __launch_bounds__(32 * kWalkWarps) k_walk(WalkArgs a) {
+    __shared__ float4 s_cell[kWalkWarps][kCellCap][3];
+    __shared__ int2 s_leaf[kWalkWarps][kLeafCap];
+    __shared__ int s_loff[kWalkWarps][kLeafCap];
+    __shared__ float4 s_part[kWalkWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned full = 0xffffffffu;
+    const unsigned lt = (1u << lane) - 1u;
+    int32_t *stk = a.queues + (size_t)(blockIdx.x * kWalkWarps + w) * kStackInts;
     const int32_t *T = a.T;
-    const int cap = a.list_cap;
-    const float4 *sp = a.poles + (size_t)dp * kPoleQ;
-    const float4 s0 = sp[0];
-    const int slot = a.list_slot[dp];
-    const int pslot = a.parent_slot[dp];
-    if (slot < 0 || slot >= a.branch_cap || pslot < 0 || pslot >= a.branch_cap) {
-        if (lane == 0) raise_health(a.health, SPH_HEALTH_LIST_CAPACITY);
-        return;
-    }
-    int32_t *out = a.list_out + (size_t)slot * cap;
-    const int32_t *in = a.list_in + (size_t)pslot * cap;
-    const float4 *lp = a.locals + (size_t)dp * kLocalQ;
-    const float4 L0 = lp[0];
-    const float lx = L0.x, ly = L0.y, lz = L0.z;
-    float acc[10];
-#pragma unroll
-    for (int j = 0; j < 10; ++j) acc[j] = 0.f;
-    int op = 0;
-    for (int c0 = 0; c0 < cap; c0 += 32) {
-        const int i = c0 + lane;
-        int e = (i < cap) ? in[i] : -1;
-        if (e < -1 || e > a.tree_cap - 10) {
-            raise_health(a.health, SPH_HEALTH_LIST_CAPACITY);
-            e = -1;
-        }
-        const uint32_t stop = __ballot_sync(0xffffffffu, e == -1);
-        const int nvalid = stop ? (__ffs(stop) - 1) : 32;
-        // bit 8: pass e itself; bits 0..7: pass child k of e
-        uint32_t pass = 0u;
-        if (lane < nvalid) {
-            const float4 *bp = a.poles + (size_t)T[e + 1] * kPoleQ;
-            const float4 b0 = bp[0];
-            if (accept_theta(lx, ly, lz, s0.w, b0, a.theta)) {
-                m2l_theta(lx, ly, lz, bp, acc);
-            } else if (T[e] != 0 || b0.w <= s0.w) {
-                pass = 1u << 8;
-            } else {
-                for (int k = 0; k < 8; ++k) {
-                    const int c = T[e + 2 + k];
-                    if (c == -1) continue;
-                    const float4 *cp = a.poles + (size_t)T[c + 1] * kPoleQ;
-                    if (accept_theta(lx, ly, lz, s0.w, cp[0], a.theta))
-                        m2l_theta(lx, ly, lz, cp, acc);
-                    else
-                        pass |= 1u << k;
-                }
+    const float soft2x4 = 4.f * kGravSoft * kGravSoft;
+    while (true) {
+        int g = 0;
+        if (lane == 0) g = (int)atomicAdd(a.counter, 1u);
+        g = __shfl_sync(full, g, 0);
+        if (g >= a.ngroups) break;
+        const int i = g * 32 + lane;
+        const bool valid = i < a.n;
+        const float4 xi = a.kp4[valid ? i : g * 32];
+        float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f, cax = 0.f, cay = 0.f, caz = 0.f, cph = 0.f;
+        int ncell = 0, nleaf = 0;
+        // the box the walk tests nodes against, and whether this lane's
+        // particle belongs to the particles being walked for
+        float bx0, by0, bz0, bx1, by1, bz1;
+        bool mine = true;
+        auto flush_cells = [&]() {
+            __syncwarp();
+            float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+            eval_cells(s_cell[w], ncell, xi, sx, sy, sz, sp);
+            if (mine) {
+                kahan_add(ax, cax, sx);
+                kahan_add(ay, cay, sy);
+                kahan_add(az, caz, sz);
+                kahan_add(ph, cph, sp);
             }
-        }
-        const int mine = __popc(pass);
-        int incl = mine;
+            ncell = 0;
+            __syncwarp();
+        };
+        auto flush_leaves = [&]() {
+            __syncwarp();
+            // number the staged leaves' particles consecutively
+            const int c0 = (lane < nleaf) ? s_leaf[w][lane].y : 0;
+            const int c1 = (lane + 32 < nleaf) ? s_leaf[w][lane + 32].y : 0;
+            int inc0 = c0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        int pos = op + incl - mine;
-        while (pass) {
-            const int k = __ffs(pass) - 1;
-            pass &= pass - 1u;
-            const int c = (k == 8) ? e : T[e + 2 + k];
-            if (pos < cap - 1) {
-                out[pos] = c;
-            } else {
-                // list full: the node is accepted although the opening test
-                // failed; the health bit tells the caller the result is degraded
-                raise_health(a.health, SPH_HEALTH_LIST_CAPACITY);
-                m2l_theta(lx, ly, lz, a.poles + (size_t)T[c + 1] * kPoleQ, acc);
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(full, inc0, o);
+                if (lane >= o) inc0 += y;
             }
-            ++pos;
-        }
-        op = min(op + total, cap - 1);
-        if (stop) break;
-    }
-    if (lane == 0) out[op] = -1;
+            const int tot0 = __shfl_sync(full, inc0, 31);
+            int inc1 = c1;
 #pragma unroll
-    for (int j = 0; j < 10; ++j) {
-        float v = acc[j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        acc[j] = v;
-    }
-    const float4 L1 = lp[1], L2 = lp[2], L3 = lp[3];
-    const float phi0 = L0.w + acc[0];
-    const float ax = L1.x + acc[1], ay = L1.y + acc[2], az = L1.z + acc[3];
-    const float txx = L1.w + acc[4], txy = L2.x + acc[5], txz = L2.y + acc[6];
-    const float tyy = L2.z + acc[7], tyz = L2.w + acc[8], tzz = L3.x + acc[9];
-    // L2L to every child, expanded about the child's centre of mass
-    if (lane < 8) {
-        const int c = T[tp + 2 + lane];
-        if (c != -1) {
-            const int cdp = T[c + 1];
-            const float4 cpos = a.poles[(size_t)cdp * kPoleQ];
-            const float sx = cpos.x - lx, sy = cpos.y - ly, sz = cpos.z - lz;
-            const float tsx = txx * sx + txy * sy + txz * sz;
-            const float tsy = txy * sx + tyy * sy + tyz * sz;
-            const float tsz = txz * sx + tyz * sy + tzz * sz;
-            const float cphi = phi0 - (ax * sx + ay * sy + az * sz) - 0.5f * (sx * tsx + sy * tsy + sz * tsz);
-            float4 *clp = a.locals + (size_t)cdp * kLocalQ;
-            clp[0] = make_float4(cpos.x, cpos.y, cpos.z, cphi);
-            clp[1] = make_float4(ax + tsx, ay + tsy, az + tsz, txx);
-            clp[2] = make_float4(txy, txz, tyy, tyz);
-            clp[3] = make_float4(tzz, 0.f, 0.f, 0.f);
-        }
-    }
-}
-
-__device__ void leaf_target(const ThetaDownArgs &a, int tp, int dp, int lane, int32_t *stk) {
-    const int32_t *T = a.T;
-    const int cap = a.list_cap;
-    const int np = T[tp];
-    const float4 s0 = a.poles[(size_t)dp * kPoleQ];
-    const int pslot = a.parent_slot[dp];
-    if (pslot < 0 || pslot >= a.branch_cap) {
-        if (lane == 0) raise_health(a.health, SPH_HEALTH_LIST_CAPACITY);
-        return;
-    }
-    const int32_t *in = a.list_in + (size_t)pslot * cap;
-    const float4 *lp = a.locals + (size_t)dp * kLocalQ;
-    const float4 L0 = lp[0], L1 = lp[1], L2 = lp[2], L3 = lp[3];
-    for (int i0 = 0; i0 < np; i0 += 32) {
-        const bool mine = i0 + lane < np;
-        const int p = mine ? T[tp + 2 + i0 + lane] : -1;
-        const float4 xi = mine ? a.pos4[p] : s0;
-        // L2P
-        const float dx = xi.x - L0.x, dy = xi.y - L0.y, dz = xi.z - L0.z;
-        const float tdx = L1.w * dx + L2.x * dy + L2.y * dz;
-        const float tdy = L2.x * dx + L2.z * dy + L2.w * dz;
-        const float tdz = L2.y * dx + L2.w * dy + L3.x * dz;
-        float ax = L1.x + tdx, ay = L1.y + tdy, az = L1.z + tdz;
-        float ph = L0.w - (L1.x * dx + L1.y * dy + L1.z * dz) - 0.5f * (dx * tdx + dy * tdy + dz * tdz);
-        float cax = 0.f, cay = 0.f, caz = 0.f, cph = 0.f;
-        int sp = 0;
-        int li = 0;
-        while (true) {
-            int e;
-            if (sp > 0) {
-                e = stk[--sp];
-            } else {
-                if (li >= cap) break;
-                e = in[li++];
-                if (e == -1) break;
-                if (e < -1 || e > a.tree_cap - 10) {
-                    if (lane == 0) raise_health(a.health, SPH_HEALTH_LIST_CAPACITY);
-                    break;
-                }
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(full, inc1, o);
+                if (lane >= o) inc1 += y;
             }
-            const float4 *bp = a.poles + (size_t)T[e + 1] * kPoleQ;
-            const float4 b0 = bp[0];
-            const int ne = T[e];
-            if (accept_theta(s0.x, s0.y, s0.z, s0.w, b0, a.theta)) {
-                const Field f = node_field(xi.x - b0.x, xi.y - b0.y, xi.z - b0.z, bp[1], bp[2]);
-                kahan_add(ax, cax, f.ax);
-                kahan_add(ay, cay, f.ay);
-                kahan_add(az, caz, f.az);
-                kahan_add(ph, cph, f.phi);
-            } else if (ne != 0) {
-                for (int j = 0; j < ne; ++j) {
-                    const int pj = T[e + 2 + j];
-                    const float4 xj = a.pos4[pj];
-                    const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-                    const float r = sqrtf(rx * rx + ry * ry + rz * rz);
-                    if (pj == p || r == 0.f) continue;
-                    float fr, pot;
-                    soft_pair(r, fr, pot);
-                    const float s = -xj.w * fr / r;
-                    kahan_add(ax, cax, s * rx);
-                    kahan_add(ay, cay, s * ry);
-                    kahan_add(az, caz, s * rz);
-                    kahan_add(ph, cph, xj.w * pot);
-                }
-            } else {
-                // open the branch: children pushed in reverse, popped in order
-                for (int k = 7; k >= 0; --k) {
-                    const int c = T[e + 2 + k];
-                    if (c == -1) continue;
-                    if (sp < kStack) {
-                        if (lane == 0) stk[sp] = c;
-                        ++sp;
-                    } else {
-                        if (lane == 0) raise_health(a.health, SPH_HEALTH_LIST_CAPACITY);
-                        const float4 *cp = a.poles + (size_t)T[c + 1] * kPoleQ;
-                        const float4 c0 = cp[0];
-                        const Field f = node_field(xi.x - c0.x, xi.y - c0.y, xi.z - c0.z, cp[1], cp[2]);
-                        kahan_add(ax, cax, f.ax);
-                        kahan_add(ay, cay, f.ay);
-                        kahan_add(az, caz, f.az);
-                        kahan_add(ph, cph, f.phi);
-                    }
+            const int tot = tot0 + __shfl_sync(full, inc1, 31);
+            if (lane < nleaf) s_loff[w][lane] = inc0 - c0;
+            if (lane + 32 < nleaf) s_loff[w][lane + 32] = tot0 + inc1 - c1;
+            __syncwarp();
+            float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+            for (int j0 = 0; j0 < tot; j0 += 32) {
+                const int j = j0 + lane;
+                if (j < tot) {
+                    int q = 0;  // the last leaf whose first particle number is <= j
+#pragma unroll
+                    for (int step = kLeafCap / 2; step > 0; step >>= 1)
+                        if (q + step < nleaf && s_loff[w][q + step] <= j) q += step;
+                    s_part[w][lane] = a.kp4[s_leaf[w][q].x + (j - s_loff[w][q])];
                 }
                 __syncwarp();
+                eval_parts(s_part[w], min(32, tot - j0), xi, sx, sy, sz, sp);
+                __syncwarp();
             }
+            if (mine) {
+                kahan_add(ax, cax, sx);
+                kahan_add(ay, cay, sy);
+                kahan_add(az, caz, sz);
+                kahan_add(ph, cph, sp);
+            }
+            nleaf = 0;
+        };
+        auto walk = [&]() {
+            // depth-first: each round pops up to 32 nodes off the top of the
+            // stack and pushes the children of the rejected branches
+            if (lane == 0) stk[0] = 0;  // the root
+            __syncwarp();
+            int size = 1;
+            while (size > 0) {
+                const int take = min(size, 32);
+                size -= take;
+                const bool v = lane < take;
+                const int tp = v ? stk[size + lane] : 0;
+                __syncwarp();
+                const int dp = T[tp + 1];
+                const int cnt = T[tp];
+                const float4 *pr = a.poles + (size_t)dp * kPoleQ;
+                const float4 c0 = pr[0];
+                const float dx = fmaxf(fmaxf(bx0 - c0.x, c0.x - bx1), 0.f);
+                const float dy = fmaxf(fmaxf(by0 - c0.y, c0.y - by1), 0.f);
+                const float dz = fmaxf(fmaxf(bz0 - c0.z, c0.z - bz1), 0.f);
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                bool acc = v && c0.w * c0.w < a.theta2 * d2 && d2 > soft2x4;
+                const bool rleaf = v && !acc && cnt != 0;
+                bool rbr = v && !acc && cnt == 0;
+                int nch = 0;
+                if (rbr)
+                    for (int c = 0; c < 8; ++c) nch += (T[tp + 2 + c] != -1) ? 1 : 0;
+                int inc = nch;
+    #pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(full, inc, o);
+                    if (lane >= o) inc += y;
+                }
+                const int tot = __shfl_sync(full, inc, 31);
+                if (size + tot > kStackInts) {
+                    // no room (deeper than the stack allows): the rejected branches
+                    // are taken as accepted nodes, flagged in the health word
+                    if (lane == 0) raise_health(a.health, SPH_HEALTH_LIST_CAPACITY);
+                    acc = acc || rbr;
+                    rbr = false;
+                } else {
+                    if (rbr) {
+                        // reversed, so that the first child is popped first
+                        int o = size + inc - 1;
+                        for (int c = 0; c < 8; ++c) {
+                            const int ch = T[tp + 2 + c];
+                            if (ch != -1) stk[o--] = ch;
+                        }
+                    }
+                    size += tot;
+                }
+                // accepted nodes: stage their records
+                if (ncell + 32 > kCellCap) flush_cells();
+                const unsigned ma = __ballot_sync(full, acc);
+                if (acc) {
+                    const int o = ncell + __popc(ma & lt);
+                    const float4 p1 = pr[1], p2 = pr[2];
+                    s_cell[w][o][0] = make_float4(c0.x, c0.y, c0.z, p1.x);
+                    s_cell[w][o][1] = make_float4(p1.y, p1.z, p1.w, p2.x);
+                    s_cell[w][o][2] = make_float4(p2.y, p2.z, 0.f, 0.f);
+                }
+                ncell += __popc(ma);
+                // rejected leaves: stage their particle ranges
+                if (nleaf + 32 > kLeafCap) flush_leaves();
+                const unsigned ml = __ballot_sync(full, rleaf);
+                if (rleaf) s_leaf[w][nleaf + __popc(ml & lt)] = a.node_range[dp];
+                nleaf += __popc(ml);
+                __syncwarp();
+            }
+            flush_cells();
+            flush_leaves();
+        };
+        // A group that straddles a jump of the key order (two distant clusters
+        // of particles) is cut there: consecutive particles farther apart
+        // than 6x the group's typical step (the mean of the steps no longer
+        // than twice the mean step) start a new segment, and every segment is
+        // walked against its own box.  Almost every group is one segment.
+        {
+            const float4 xn = make_float4(__shfl_down_sync(full, xi.x, 1), __shfl_down_sync(full, xi.y, 1),
+                                          __shfl_down_sync(full, xi.z, 1), 0.f);
+            const bool has_next = lane < 31;
+            const float ddx = xn.x - xi.x, ddy = xn.y - xi.y, ddz = xn.z - xi.z;
+            const float step = has_next ? sqrtf(ddx * ddx + ddy * ddy + ddz * ddz) : 0.f;
+            const float mean1 = warp_reduce_sum(step) * (1.f / 31.f);
+            const bool small = has_next && step <= 2.f * mean1;
+            const float n2 = warp_reduce_sum(small ? 1.f : 0.f);
+            const float mean2 = warp_reduce_sum(small ? step : 0.f) / fmaxf(n2, 1.f);
+            const bool cut = has_next && step > 6.f * mean2 && step > 0.f;
+            // segment of this lane = number of cuts before it
+            const unsigned cuts = __ballot_sync(full, cut);
+            const int seg = __popc(cuts & lt);
+            const int nseg = __popc(cuts) + 1;
+            for (int q = 0; q < nseg; ++q) {
+                mine = seg == q;
+                const float big = 3.402823466e+38f;
+                bx0 = warp_reduce_min(mine ? xi.x : big);
+                by0 = warp_reduce_min(mine ? xi.y : big);
+                bz0 = warp_reduce_min(mine ? xi.z : big);
+                bx1 = warp_reduce_max(mine ? xi.x : -big);
+                by1 = warp_reduce_max(mine ? xi.y : -big);
+                bz1 = warp_reduce_max(mine ? xi.z : -big);
+                walk();
+            }
+        }
+        if (valid) {
+            const uint32_t id = a.order[i];
+            const float4 old = a.acc4[id];
+            a.acc4[id] = make_float4(kG * ax, kG * ay, kG * az, old.w);
+            a.gnorm[id] = sqrtf(ax * ax + ay * ay + az * az);
+            a.phi[id] = kG * ph;
         }
         __syncwarp();
-        if (mine) {
-            const float4 old = a.acc4[p];
-            a.acc4[p] = make_float4(kG * ax, kG * ay, kG * az, old.w);
-            a.gnorm[p] = sqrtf(ax * ax + ay * ay + az * az);
-            a.phi[p] = kG * ph;
-        }
     }
 }
-
-constexpr int kDownWarps = 4;
-
-__global__ void __launch_bounds__(32 * kDownWarps) k_down_theta(ThetaDownArgs a, int level, int64_t level_cap) {
-    __shared__ int32_t stacks[kDownWarps][kStack];
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    const int warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const int cnt = a.level_count[level];
-    const int32_t *nodes = a.level_nodes + (size_t)level * level_cap;
-    const int32_t *T = a.T;
-    for (int t = warp0; t < cnt; t += nwarps) {
-        const int tp = nodes[t];
-        if (tp == 0) {
-            if (T[0] != 0) {
-                if (lane == 0) raise_health(a.health, SPH_HEALTH_ROOT_LEAF);
-                continue;
-            }
-            // the root: zero locals at its children's centres, list = [root]
-            if (lane < 8) {
-                const int c = T[2 + lane];
-                if (c != -1) {
-                    const int cdp = T[c + 1];
-                    const float4 cp = a.poles[(size_t)cdp * kPoleQ];
-                    float4 *lp = a.locals + (size_t)cdp * kLocalQ;
-                    lp[0] = make_float4(cp.x, cp.y, cp.z, 0.f);
-                    lp[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    lp[2] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    lp[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            }
-            if (lane == 0) {
-                a.list_out[0] = 0;
-                a.list_out[1] = -1;
-            }
-            continue;
-        }
-        const int dp = T[tp + 1];
-        if (T[tp] == 0)
-            branch_target(a, tp, dp, lane);
-        else
-            leaf_target(a, tp, dp, lane, stacks[wib]);
-    }
-}
-
 // FP64 direct sum over all particles at the given targets, with the exact
 // softened kernel: out[4 t] = (ax, ay, az, phi) including G.  One block per
 // target; positions are the float32 working positions promoted to double.
@@ -594,7 +555,13 @@ __global__ void __launch_bounds__(256) k_direct_f64(const float4 *__restrict__ p
 
 sph_status launch_gravity_theta(sph_ctx *ctx, cudaStream_t st) {
     Tree &tr = ctx->tree;
+    TreeBuild &tb = ctx->tb;
     if (!tr.valid || ctx->n <= 0) return SPH_OK;
+    if (ctx->params.tree_source != SPH_TREE_GPU || !tb.order) {
+        set_error("the theta gravity form walks the GPU-built tree (tree_source SPH_TREE_GPU)");
+        return SPH_ERR_UNSUPPORTED;
+    }
+    const int n = ctx->n;
     const int L = tr.n_levels_host;
     ThetaUpArgs u;
     u.T = tr.tree;
@@ -611,31 +578,49 @@ sph_status launch_gravity_theta(sph_ctx *ctx, cudaStream_t st) {
         blocks = blocks < 1 ? 1 : (blocks > 148 * 32 ? 148 * 32 : blocks);
         k_up_theta<<<blocks, 128, 0, st>>>(u, l, tr.level_cap);
     }
-    ThetaDownArgs d;
-    d.T = tr.tree;
-    d.level_nodes = tr.level_nodes;
-    d.level_count = tr.level_count;
-    d.list_slot = tr.list_slot;
-    d.parent_slot = tr.parent_slot;
-    d.poles = tr.poles;
-    d.locals = tr.locals;
-    d.list_cap = tr.list_cap;
-    d.branch_cap = tr.branch_cap;
-    d.tree_cap = tr.tree_cap;
-    d.theta = ctx->form.theta;
-    d.pos4 = ctx->pos4;
-    d.acc4 = ctx->acc4;
-    d.gnorm = ctx->gnorm;
-    d.phi = ctx->phi;
-    d.health = ctx->health;
-    for (int l = 0; l < L; ++l) {
-        d.list_in = (l % 2 == 0) ? tr.lists[0] : tr.lists[1];
-        d.list_out = (l % 2 == 0) ? tr.lists[1] : tr.lists[0];
-        int64_t bound = tr.level_count_host[l];
-        int blocks = (int)((bound * 32 + 32 * kDownWarps - 1) / (32 * kDownWarps));
-        blocks = blocks < 1 ? 1 : (blocks > 148 * 32 ? 148 * 32 : blocks);
-        k_down_theta<<<blocks, 32 * kDownWarps, 0, st>>>(d, l, tr.level_cap);
+    // resident warps of the walk, each with its two node queues
+    static int max_blocks_per_sm = 0;
+    if (max_blocks_per_sm == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_blocks_per_sm, k_walk, 32 * kWalkWarps, 0);
+        if (max_blocks_per_sm < 1) max_blocks_per_sm = 1;
     }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    const int ngroups = (n + 31) / 32;
+    int blocks = sms * max_blocks_per_sm;
+    if (blocks * kWalkWarps > ngroups) blocks = (ngroups + kWalkWarps - 1) / kWalkWarps;
+    const int64_t qints = (int64_t)blocks * kWalkWarps * kStackInts;
+    if (qints > tb.walk_queue_ints) {
+        cudaFree(tb.walk_queues);
+        tb.walk_queues = nullptr;
+        tb.walk_queue_ints = 0;
+        cudaError_t e = cudaMalloc(&tb.walk_queues, sizeof(int32_t) * qints);
+        if (e != cudaSuccess) return cuda_status(e, "gravity (theta) walk queues");
+        tb.walk_queue_ints = qints;
+    }
+    if (!tb.walk_counter) {
+        cudaError_t e = cudaMalloc(&tb.walk_counter, sizeof(uint32_t));
+        if (e != cudaSuccess) return cuda_status(e, "gravity (theta) walk counter");
+    }
+    float4 *kp4 = ctx->sp4;  // free until the density pass gathers its own records
+    k_gather_key_order<<<(n + 255) / 256, 256, 0, st>>>(n, tb.order, ctx->pos4, kp4);
+    cudaMemsetAsync(tb.walk_counter, 0, sizeof(uint32_t), st);
+    WalkArgs w;
+    w.T = tr.tree;
+    w.poles = tr.poles;
+    w.node_range = tr.node_range;
+    w.kp4 = kp4;
+    w.order = tb.order;
+    w.n = n;
+    w.ngroups = ngroups;
+    w.theta2 = ctx->form.theta * ctx->form.theta;
+    w.acc4 = ctx->acc4;
+    w.gnorm = ctx->gnorm;
+    w.phi = ctx->phi;
+    w.queues = tb.walk_queues;
+    w.counter = tb.walk_counter;
+    w.health = ctx->health;
+    k_walk<<<blocks, 32 * kWalkWarps, 0, st>>>(w);
     return cuda_status(cudaGetLastError(), "gravity (theta)");
 }
 

@@ -53,6 +53,7 @@ struct Tree {
     float4 *locals = nullptr;       // [node_cap][kLocalQ]
     int32_t *lists[2] = {nullptr, nullptr}; // unchecked-node lists, [branch_cap][list_cap] each
     int32_t *meta = nullptr;        // device: [0] n_levels, [1] n_nodes, [2] tree_len
+    int2 *node_range = nullptr;     // [node_cap] by data pointer: (first, count) in the GPU tree's key order
     int64_t node_cap = 0;
     int64_t level_cap = 0;
     int64_t branch_cap = 0;         // list slots per level
@@ -77,6 +78,10 @@ struct TreeBuild {
     int32_t *ndp = nullptr;     // [max_levels][level_cap] data pointer
     float *bbox = nullptr;      // device [6] lo.xyz, hi.xyz as ordered ints
     int64_t scan_cap = 0;
+    const uint32_t *order = nullptr;  // particle ids in the tree's key order (last GPU build)
+    int32_t *walk_queues = nullptr;   // theta-form walk: node queues of the resident warps
+    uint32_t *walk_counter = nullptr; // theta-form walk: group ticket
+    int64_t walk_queue_ints = 0;
 };
 
 }  // namespace sph

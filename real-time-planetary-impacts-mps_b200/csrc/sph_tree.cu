@@ -196,6 +196,7 @@ struct LayoutArgs {
     int32_t *first_level;
     const int64_t *ints_off, *dp_off;
     int32_t *tree, *level_nodes, *list_slot;
+    int2 *node_range;  // by data pointer: (first particle in key order, count)
     const uint32_t *order;
     int depth, leafcap, n;
     int64_t tree_cap, node_cap;
@@ -252,6 +253,7 @@ __global__ void k_write(LayoutArgs a, int l) {
             for (int k = 0; k < c; ++k) T[2 + k] = (int32_t)a.order[s + k];
         }
         a.list_slot[dp] = br ? a.nrank[base + t] : -1;
+        a.node_range[dp] = make_int2(s, c);
     }
     if (l == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
         a.meta[1] = (int32_t)a.dp_off[a.n];
@@ -318,6 +320,8 @@ void tree_free(sph_ctx *ctx) {
     cudaFree(tb.scan_blocks);
     cudaFree(tb.per_particle);
     cudaFree(tb.bbox);
+    cudaFree(tb.walk_queues);
+    cudaFree(tb.walk_counter);
     tb = TreeBuild();
 }
 
@@ -399,6 +403,8 @@ sph_status launch_tree_build(sph_ctx *ctx, cudaStream_t st) {
     ya.node_cap = tr.node_cap;
     ya.health = ctx->health;
     ya.meta = tr.meta;
+    ya.node_range = tr.node_range;
+    tb.order = order;
     k_layout_reset<<<grid_for(n + 1), 256, 0, st>>>(ya);
     int64_t lb[16];
     bound = 1;
