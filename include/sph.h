@@ -149,15 +149,23 @@ sph_status sph_step(sph_ctx *ctx, void *stream);         /* Compute::stepPass (:
  * reference; the default form (all zero) reproduces the reference's logic,
  * quirks included, and is what the parity tests check against it. */
 #define SPH_GRAVITY_REFERENCE 0 /* adaptive acceptance, forced leaf M2L, truncated softening (Compute.cpp:328-377) */
-#define SPH_GRAVITY_THETA     1 /* opening angle theta, quadrupole M2L/M2P, exact softened P2P, Kahan sums */
+#define SPH_GRAVITY_THETA     1 /* opening-angle group walk: quadrupole M2P, exact softened P2P, Kahan sums;
+                                   needs the GPU-built tree (SPH_TREE_GPU) */
+#define SPH_PRECISION_REFERENCE 0 /* float positions drifted in float, as the reference (step.metal:45) */
+#define SPH_PRECISION_MIXED     1 /* FP64 master positions and global time (float working copies), Kahan-
+                                     compensated acceleration, du/dt and dh/dt sums */
 typedef struct {
-    int32_t gravity; /* SPH_GRAVITY_* */
-    float theta;     /* opening angle of SPH_GRAVITY_THETA: accept when r_A + r_B < theta |com_A - com_B| */
-    int32_t h_seed;  /* reserved, 0 */
-    int32_t precision; /* reserved, 0 */
+    int32_t gravity;   /* SPH_GRAVITY_* */
+    float theta;       /* opening angle of SPH_GRAVITY_THETA: a node of radius r_node (about its centre of
+                          mass) is accepted for a group of particles when r_node < theta d, d = the distance
+                          from its centre of mass to the group's bounding box, and d > 2 x softening */
+    int32_t h_seed;    /* reserved, 0 */
+    int32_t precision; /* SPH_PRECISION_* */
 } sph_form;
 void sph_form_default(sph_form *f); /* reference form, theta 0.5 */
-/* Select the form for the following passes (drops a captured step graph). */
+/* Select the form for the following passes (drops a captured step graph).
+ * Entering SPH_PRECISION_MIXED takes the current float positions as the FP64
+ * master positions and the current global time as the FP64 time. */
 sph_status sph_set_form(sph_ctx *ctx, const sph_form *f);
 sph_status sph_get_form(const sph_ctx *ctx, sph_form *f);
 
@@ -168,6 +176,24 @@ sph_status sph_get_form(const sph_ctx *ctx, sph_form *f);
  * gravity forms; no counterpart in the reference.  Synchronous. */
 sph_status sph_gravity_direct_f64(sph_ctx *ctx, const int32_t *targets, int32_t n_targets, double *out,
                                   void *stream);
+
+/* FP64 conservation diagnostics (no counterpart in the reference, which
+ * computes no potential: L2P.metal:12-32 returns only the acceleration).
+ * Sums over all particles in FP64, in a fixed order: mass, kinetic energy
+ * 1/2 m v^2, internal energy m u, potential energy 1/2 m phi, momentum m v and
+ * angular momentum m x v about the origin (FP64 positions in the mixed form).
+ * phi is evaluated for the current positions by the opening-angle walk at
+ * theta_potential (0 = 0.5) on a freshly built GPU tree, without touching the
+ * accelerations; with a host tree (SPH_TREE_HOST) no potential is computed
+ * and potential_valid is 0.  Synchronous on `stream`. */
+typedef struct {
+    double mass, kinetic, internal, potential, total;
+    double momentum[3], angular_momentum[3];
+    double time;             /* global time, seconds (FP64 in the mixed form) */
+    int32_t potential_valid;
+    uint32_t health;         /* the device health word */
+} sph_diag;
+sph_status sph_diagnostics(sph_ctx *ctx, void *stream, float theta_potential, sph_diag *out);
 
 /* Cell sort for callers that cannot allocate device memory.  No counterpart in
  * the reference.  Meant for code whose host framework owns every device

@@ -73,6 +73,17 @@ class SphForm(C.Structure):
     _fields_ = [("gravity", C.c_int32), ("theta", C.c_float), ("h_seed", C.c_int32), ("precision", C.c_int32)]
 
 
+SPH_PRECISION_REFERENCE = 0
+SPH_PRECISION_MIXED = 1
+
+
+class SphDiag(C.Structure):
+    _fields_ = [("mass", C.c_double), ("kinetic", C.c_double), ("internal", C.c_double),
+                ("potential", C.c_double), ("total", C.c_double), ("momentum", C.c_double * 3),
+                ("angular_momentum", C.c_double * 3), ("time", C.c_double), ("potential_valid", C.c_int32),
+                ("health", C.c_uint32)]
+
+
 class SphError(RuntimeError):
     def __init__(self, status: int, what: str, detail: str = ""):
         self.status = status
@@ -160,6 +171,7 @@ def load(parity: bool = False) -> C.CDLL:
         "sph_set_form": (st, [vp, C.POINTER(SphForm)]),
         "sph_get_form": (st, [vp, C.POINTER(SphForm)]),
         "sph_gravity_direct_f64": (st, [vp, _ip, C.c_int32, C.POINTER(C.c_double), vp]),
+        "sph_diagnostics": (st, [vp, vp, C.c_float, C.POINTER(SphDiag)]),
         "sph_draw_snapshot": (st, [vp, vp, _ip]),
         "sph_upload": (st, [vp, C.c_int, vp, C.c_size_t]),
         "sph_download": (st, [vp, C.c_int, vp, C.c_size_t]),

@@ -176,19 +176,32 @@ class Compute:
                     n_levels=nl.value, n_nodes=nn.value)
 
     # ---- numerical forms (no reference counterpart) --------------------
-    def set_form(self, gravity: str = "reference", theta: float = 0.5):
-        """Select the gravity form: "reference" (the reference's logic) or
-        "theta" (opening-angle FMM with exact near field)."""
+    def set_form(self, gravity: str = "reference", theta: float = 0.5, precision: str = "reference"):
+        """Select the numerical form: gravity "reference" (the reference's
+        logic) or "theta" (opening-angle group walk with exact near field);
+        precision "reference" (float positions) or "mixed" (FP64 master
+        positions and time, Kahan-compensated sums)."""
         f = _lib.SphForm()
         self._lib.sph_form_default(C.byref(f))
         f.gravity = _lib.SPH_GRAVITY_THETA if gravity == "theta" else _lib.SPH_GRAVITY_REFERENCE
         f.theta = float(theta)
+        f.precision = _lib.SPH_PRECISION_MIXED if precision == "mixed" else _lib.SPH_PRECISION_REFERENCE
         self._check(self._lib.sph_set_form(self._h, C.byref(f)), "sph_set_form")
 
     def get_form(self) -> dict:
         f = _lib.SphForm()
         self._check(self._lib.sph_get_form(self._h, C.byref(f)), "sph_get_form")
-        return dict(gravity="theta" if f.gravity == _lib.SPH_GRAVITY_THETA else "reference", theta=f.theta)
+        return dict(gravity="theta" if f.gravity == _lib.SPH_GRAVITY_THETA else "reference", theta=f.theta,
+                    precision="mixed" if f.precision == _lib.SPH_PRECISION_MIXED else "reference")
+
+    def diagnostics(self, stream=None, theta_potential: float = 0.5) -> dict:
+        """FP64 conservation sums (mass, energies, momentum, angular momentum)."""
+        d = _lib.SphDiag()
+        self._check(self._lib.sph_diagnostics(self._h, _stream(stream), float(theta_potential), C.byref(d)),
+                    "sph_diagnostics")
+        return dict(mass=d.mass, kinetic=d.kinetic, internal=d.internal, potential=d.potential, total=d.total,
+                    momentum=list(d.momentum), angular_momentum=list(d.angular_momentum), time=d.time,
+                    potential_valid=bool(d.potential_valid), health=d.health)
 
     def gravity_direct_f64(self, targets, stream=None) -> np.ndarray:
         """FP64 direct-sum (ax, ay, az, phi) at the given particles, G included."""

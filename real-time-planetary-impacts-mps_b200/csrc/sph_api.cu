@@ -53,6 +53,9 @@ __global__ void k_get_w(const float4 *__restrict__ src, float *__restrict__ dst,
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = src[i].w;
 }
+__global__ void k_time_to64(const int32_t *globals, double *dglob) {
+    dglob[0] = (double)kDtMin1 * (double)globals[0];
+}
 __global__ void k_split_cells(const uint2 *__restrict__ src, uint32_t *__restrict__ dst, uint32_t count, int which) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
         dst[i] = which ? src[i].y : src[i].x;
@@ -270,7 +273,8 @@ sph_status sph_destroy(sph_ctx *ctx) {
     void *bufs[] = {ctx->pos4, ctx->vel4, ctx->acc4, ctx->rho, ctx->u, ctx->P, ctx->h, ctx->f, ctx->c,
                     ctx->du, ctx->B, ctx->dhdt, ctx->gnorm, ctx->phi, ctx->mat, ctx->nat, ctx->active, ctx->globals,
                     ctx->health, ctx->cell_range, ctx->sp4, ctx->sv4, ctx->sA, ctx->sB, ctx->sC,
-                    ctx->eos_forsterite, ctx->eos_fe, ctx->stage, ctx->snapshot};
+                    ctx->eos_forsterite, ctx->eos_fe, ctx->stage, ctx->snapshot, ctx->pos64, ctx->dglob,
+                    ctx->diag};
     for (void *b : bufs) cudaFree(b);
     sort_free(ctx->cell_sort);
     tree_free(ctx);
@@ -343,6 +347,8 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     ctx->stage_bytes = std::max((size_t)kNumCells * sizeof(uint32_t), sizeof(float) * 3 * (size_t)n);
     chk(cudaMalloc(&ctx->stage, ctx->stage_bytes));
     chk(dmalloc(&ctx->snapshot, (size_t)kSnapshotRes * kSnapshotRes));
+    chk(dmalloc(&ctx->dglob, 4));
+    chk(dmalloc(&ctx->diag, (size_t)kDiagDoubles));
     if (e != cudaSuccess) {
         s = cuda_status(e, "sph_create allocation");
         sph_destroy(ctx);
@@ -377,6 +383,7 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     chk(cudaMemset(ctx->active, 1, n));
     chk(cudaMemset(ctx->nat, 0, sizeof(int32_t) * n));
     chk(cudaMemset(ctx->globals, 0, sizeof(int32_t) * 4));
+    chk(cudaMemset(ctx->dglob, 0, sizeof(double) * 4));
     chk(cudaMemset(ctx->health, 0, sizeof(uint32_t)));
     if (e != cudaSuccess) {
         s = cuda_status(e, "sph_create init");
@@ -437,6 +444,8 @@ sph_status sph_upload_async(sph_ctx *ctx, sph_field field, const void *host, siz
                 k_pack3<<<blocks, 256, 0, st>>>((const float *)ctx->stage, dst, n, field == SPH_FIELD_POS ? 1 : 0);
                 e = cudaGetLastError();
             }
+            if (e == cudaSuccess && field == SPH_FIELD_POS && ctx->form.precision == SPH_PRECISION_MIXED)
+                return launch_pos_to64(ctx, st);
             return cuda_status(e, "sph_upload");
         }
         case SPH_FIELD_MASS: {
@@ -803,8 +812,16 @@ sph_status sph_set_form(sph_ctx *ctx, const sph_form *f) {
         set_error("sph_set_form: theta = %g is outside (0, 1.5]", (double)f->theta);
         return SPH_ERR_INVALID_ARG;
     }
-    if (f->h_seed != 0 || f->precision != 0) {
-        set_error("sph_set_form: h_seed and precision must be 0");
+    if (f->h_seed != 0) {
+        set_error("sph_set_form: h_seed must be 0");
+        return SPH_ERR_UNSUPPORTED;
+    }
+    if (f->precision != SPH_PRECISION_REFERENCE && f->precision != SPH_PRECISION_MIXED) {
+        set_error("sph_set_form: precision = %d is not a SPH_PRECISION_* value", (int)f->precision);
+        return SPH_ERR_INVALID_ARG;
+    }
+    if (f->gravity == SPH_GRAVITY_THETA && ctx->params.tree_source != SPH_TREE_GPU) {
+        set_error("sph_set_form: the theta gravity form needs the GPU-built tree (SPH_TREE_GPU)");
         return SPH_ERR_UNSUPPORTED;
     }
     cudaSetDevice(ctx->device);
@@ -812,7 +829,20 @@ sph_status sph_set_form(sph_ctx *ctx, const sph_form *f) {
         cudaGraphExecDestroy(ctx->graph);
         ctx->graph = nullptr;
     }
+    const bool enter_mixed = f->precision == SPH_PRECISION_MIXED && ctx->form.precision != SPH_PRECISION_MIXED;
     ctx->form = *f;
+    if (enter_mixed) {
+        cudaError_t e = cudaSuccess;
+        if (!ctx->pos64) e = cudaMalloc(&ctx->pos64, sizeof(double4) * (size_t)ctx->n);
+        if (e != cudaSuccess) {
+            ctx->form.precision = SPH_PRECISION_REFERENCE;
+            return cuda_status(e, "sph_set_form: FP64 positions");
+        }
+        sph_status s = launch_pos_to64(ctx, nullptr);
+        if (s != SPH_OK) return s;
+        k_time_to64<<<1, 1>>>(ctx->globals, ctx->dglob);
+        return cuda_status(cudaDeviceSynchronize(), "sph_set_form");
+    }
     return SPH_OK;
 }
 
@@ -852,6 +882,49 @@ sph_status sph_gravity_direct_f64(sph_ctx *ctx, const int32_t *targets, int32_t 
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     return cuda_status(e, "sph_gravity_direct_f64");
 }
+sph_status sph_diagnostics(sph_ctx *ctx, void *stream, float theta_potential, sph_diag *out) {
+    if (!ctx || !out) return SPH_ERR_INVALID_ARG;
+    if (!(theta_potential >= 0.f && theta_potential <= 1.5f)) {
+        set_error("sph_diagnostics: theta_potential = %g is outside [0, 1.5]", (double)theta_potential);
+        return SPH_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    std::memset(out, 0, sizeof(*out));
+    sph_status s = SPH_OK;
+    const bool pot = ctx->params.tree_source == SPH_TREE_GPU;
+    if (pot) {
+        s = launch_tree_build(ctx, st);
+        if (s == SPH_OK) s = launch_potential_theta(ctx, theta_potential > 0.f ? theta_potential : 0.5f, st);
+    } else {
+        cudaMemsetAsync(ctx->phi, 0, sizeof(float) * (size_t)ctx->n, st);
+    }
+    if (s == SPH_OK) s = launch_diag_sums(ctx, st);
+    if (s != SPH_OK) return s;
+    double tot[kDiag];
+    int32_t g[2] = {0, 0};
+    double t64 = 0.0;
+    cudaError_t e = cudaMemcpyAsync(tot, ctx->diag + (size_t)kDiagBlocks * kDiag, sizeof(tot), cudaMemcpyDeviceToHost,
+                                    st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(g, ctx->globals, sizeof(g), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&t64, ctx->dglob, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&out->health, ctx->health, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e, "sph_diagnostics");
+    out->mass = tot[0];
+    out->kinetic = tot[1];
+    out->internal = tot[2];
+    out->potential = pot ? tot[3] : 0.0;
+    out->total = out->kinetic + out->internal + out->potential;
+    for (int k = 0; k < 3; ++k) {
+        out->momentum[k] = tot[4 + k];
+        out->angular_momentum[k] = tot[7 + k];
+    }
+    out->time = ctx->form.precision == SPH_PRECISION_MIXED ? t64 : (double)kDtMin1 * (double)g[0];
+    out->potential_valid = pot ? 1 : 0;
+    return SPH_OK;
+}
+
 sph_status sph_density(sph_ctx *ctx, void *stream) {
     return ctx ? launch_density(ctx, (cudaStream_t)stream) : SPH_ERR_INVALID_ARG;
 }

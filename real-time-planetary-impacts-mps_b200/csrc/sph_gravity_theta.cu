@@ -298,6 +298,7 @@ __device__ __forceinline__ void eval_parts(const float4 *part, int np, float4 x,
     }
 }
 
+template <bool ACC>
 __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(WalkArgs a) {
     __shared__ float4 s_cell[kWalkWarps][kCellCap][3];
     __shared__ int2 s_leaf[kWalkWarps][kLeafCap];
@@ -485,9 +486,11 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(WalkArgs a) {
         }
         if (valid) {
             const uint32_t id = a.order[i];
-            const float4 old = a.acc4[id];
-            a.acc4[id] = make_float4(kG * ax, kG * ay, kG * az, old.w);
-            a.gnorm[id] = sqrtf(ax * ax + ay * ay + az * az);
+            if (ACC) {
+                const float4 old = a.acc4[id];
+                a.acc4[id] = make_float4(kG * ax, kG * ay, kG * az, old.w);
+                a.gnorm[id] = sqrtf(ax * ax + ay * ay + az * az);
+            }
             a.phi[id] = kG * ph;
         }
         __syncwarp();
@@ -553,7 +556,7 @@ __global__ void __launch_bounds__(256) k_direct_f64(const float4 *__restrict__ p
 
 }  // namespace
 
-sph_status launch_gravity_theta(sph_ctx *ctx, cudaStream_t st) {
+static sph_status theta_pass(sph_ctx *ctx, float theta, bool acc, cudaStream_t st) {
     Tree &tr = ctx->tree;
     TreeBuild &tb = ctx->tb;
     if (!tr.valid || ctx->n <= 0) return SPH_OK;
@@ -581,7 +584,10 @@ sph_status launch_gravity_theta(sph_ctx *ctx, cudaStream_t st) {
     // resident warps of the walk, each with its two node queues
     static int max_blocks_per_sm = 0;
     if (max_blocks_per_sm == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_blocks_per_sm, k_walk, 32 * kWalkWarps, 0);
+        int b0 = 0, b1 = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_walk<true>, 32 * kWalkWarps, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_walk<false>, 32 * kWalkWarps, 0);
+        max_blocks_per_sm = b0 < b1 ? b0 : b1;
         if (max_blocks_per_sm < 1) max_blocks_per_sm = 1;
     }
     int sms = 148;
@@ -613,15 +619,24 @@ sph_status launch_gravity_theta(sph_ctx *ctx, cudaStream_t st) {
     w.order = tb.order;
     w.n = n;
     w.ngroups = ngroups;
-    w.theta2 = ctx->form.theta * ctx->form.theta;
+    w.theta2 = theta * theta;
     w.acc4 = ctx->acc4;
     w.gnorm = ctx->gnorm;
     w.phi = ctx->phi;
     w.queues = tb.walk_queues;
     w.counter = tb.walk_counter;
     w.health = ctx->health;
-    k_walk<<<blocks, 32 * kWalkWarps, 0, st>>>(w);
+    if (acc)
+        k_walk<true><<<blocks, 32 * kWalkWarps, 0, st>>>(w);
+    else
+        k_walk<false><<<blocks, 32 * kWalkWarps, 0, st>>>(w);
     return cuda_status(cudaGetLastError(), "gravity (theta)");
+}
+
+sph_status launch_gravity_theta(sph_ctx *ctx, cudaStream_t st) { return theta_pass(ctx, ctx->form.theta, true, st); }
+
+sph_status launch_potential_theta(sph_ctx *ctx, float theta, cudaStream_t st) {
+    return theta_pass(ctx, theta, false, st);
 }
 
 sph_status launch_direct_f64(sph_ctx *ctx, const int32_t *d_targets, int nt, double *d_out, cudaStream_t st) {

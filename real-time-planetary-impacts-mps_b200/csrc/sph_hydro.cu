@@ -450,7 +450,7 @@ struct AccelArgs {
 // seen, Q8).  The pairs that pass the reference's test are first collected in
 // order into the group's list, then evaluated by all lanes of the group
 // together, so the long pair computation runs with every lane busy.
-template <int L>
+template <int L, bool KAHAN>
 __global__ void __launch_bounds__(parts_per_block<L>() * L) k_acceleration(AccelArgs a) {
     extern __shared__ uint32_t s_lists[];
     __shared__ uint32_t s_off[parts_per_block<L>() * L], s_start[parts_per_block<L>() * L];
@@ -472,8 +472,20 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_acceleration(Accel
             const float hi1 = 1.f / hi;
             const float hi2x4 = hi * hi * 4.f;
             float dvx = 0.f, dvy = 0.f, dvz = 0.f, du = 0.f, dh = 0.f;
+            // compensations of the Kahan sums (mixed-precision form)
+            float kx = 0.f, ky = 0.f, kz = 0.f, ku = 0.f, kh = 0.f;
             float vsig_i = 1e-12f;
             const float4 *sA = a.sA, *sB = a.sB, *sC = a.sC;
+            auto add = [&](float &sum, float &comp, float v) {
+                if (KAHAN) {
+                    const float y = v - comp;
+                    const float t = sum + y;
+                    comp = (t - sum) - y;
+                    sum = t;
+                } else {
+                    sum += v;
+                }
+            };
             auto pair = [&](uint32_t k) {
                 const float4 Aj = __ldg(sA + k);
                 const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
@@ -498,11 +510,11 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_acceleration(Accel
                 const float gix = si * rhx, giy = si * rhy, giz = si * rhz;
                 const float gjx = sj * rhx, gjy = sj * rhy, gjz = sj * rhz;
                 const float gx = 0.5f * (gix + gjx), gy = 0.5f * (giy + gjy), gz = 0.5f * (giz + gjz);
-                dvx -= mj * (facti * gix + factj * gjx + nu * gx);
-                dvy -= mj * (facti * giy + factj * gjy + nu * gy);
-                dvz -= mj * (facti * giz + factj * gjz + nu * gz);
-                du += mj * (facti * (vx * gix + vy * giy + vz * giz) + 0.5f * nu * (vx * gx + vy * gy + vz * gz));
-                dh += (mj / rhoj) * (vx * gix + vy * giy + vz * giz);
+                add(dvx, kx, -(mj * (facti * gix + factj * gjx + nu * gx)));
+                add(dvy, ky, -(mj * (facti * giy + factj * gjy + nu * gy)));
+                add(dvz, kz, -(mj * (facti * giz + factj * gjz + nu * gz)));
+                add(du, ku, mj * (facti * (vx * gix + vy * giy + vz * giz) + 0.5f * nu * (vx * gx + vy * gy + vz * gz)));
+                add(dh, kh, (mj / rhoj) * (vx * gix + vy * giy + vz * giz));
             };
             auto drain = [&](int cnt) {
                 __syncwarp(gm);
@@ -522,6 +534,13 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_acceleration(Accel
                 },
                 drain);
             drain(rest);
+            if (KAHAN) {
+                dvx -= kx;
+                dvy -= ky;
+                dvz -= kz;
+                du -= ku;
+                dh -= kh;
+            }
             dvx = group_sum<L>(dvx, gm);
             dvy = group_sum<L>(dvy, gm);
             dvz = group_sum<L>(dvz, gm);
@@ -567,16 +586,24 @@ struct StepArgs {
     float *rho, *u, *h;
     const float *du, *dhdt;
     int32_t *globals;
+    double4 *pos64;  // mixed-precision form: FP64 master positions
+    double *dglob;   // mixed-precision form: [0] global time in seconds
 };
 
 // step.metal:12-46.  Every thread reads dt before thread 0 advances the
-// global time in a separate word, as in the reference.
+// global time in a separate word, as in the reference.  MIXED: the drift is
+// added to FP64 positions, and the float positions are their roundings; the
+// global time is also kept in FP64 seconds.
+template <bool MIXED>
 __global__ void k_step(StepArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int32_t ticks = a.globals[1];
     const float dt = kDtMin1 * (float)ticks;
-    if (i == 0) a.globals[0] += ticks;
+    if (i == 0) {
+        a.globals[0] += ticks;
+        if (MIXED) a.dglob[0] += (double)kDtMin1 * (double)ticks;
+    }
     float4 v = a.vel4[i];
     const float4 ac = a.acc4[i];
     const float hi = a.h[i];
@@ -587,10 +614,90 @@ __global__ void k_step(StepArgs a) {
     a.vel4[i] = make_float4(v.x + dt * ac.x, v.y + dt * ac.y, v.z + dt * ac.z, v.w);
     a.u[i] += dt * a.du[i];
     float4 p = a.pos4[i];
-    p.x += dt * v.x + 0.5f * ac.x * dt * dt;
-    p.y += dt * v.y + 0.5f * ac.y * dt * dt;
-    p.z += dt * v.z + 0.5f * ac.z * dt * dt;
+    const float dx = dt * v.x + 0.5f * ac.x * dt * dt;
+    const float dy = dt * v.y + 0.5f * ac.y * dt * dt;
+    const float dz = dt * v.z + 0.5f * ac.z * dt * dt;
+    if (MIXED) {
+        double4 q = a.pos64[i];
+        q.x += (double)dx;
+        q.y += (double)dy;
+        q.z += (double)dz;
+        a.pos64[i] = q;
+        p.x = (float)q.x;
+        p.y = (float)q.y;
+        p.z = (float)q.z;
+    } else {
+        p.x += dx;
+        p.y += dy;
+        p.z += dz;
+    }
     a.pos4[i] = p;
+}
+
+__global__ void k_pos_to64(int n, const float4 *__restrict__ pos4, double4 *__restrict__ pos64) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos4[i];
+    pos64[i] = make_double4((double)p.x, (double)p.y, (double)p.z, 0.0);
+}
+
+// FP64 conservation sums per block: mass, kinetic, internal and potential
+// energy, momentum, angular momentum about the origin (FP64 positions when
+// present); one record of kDiag doubles per block, summed in block order by
+// k_diag_total so the result does not depend on scheduling.
+constexpr int kDiagThreads = 256;
+__global__ void __launch_bounds__(kDiagThreads) k_diag_block(int n, const float4 *__restrict__ pos4,
+                                                                const double4 *__restrict__ pos64,
+                                                                const float4 *__restrict__ vel4,
+                                                                const float *__restrict__ u,
+                                                                const float *__restrict__ phi, double *out) {
+    __shared__ double red[kDiag][kDiagThreads / 32];
+    double v[kDiag];
+#pragma unroll
+    for (int k = 0; k < kDiag; ++k) v[k] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = pos4[i];
+        const double m = (double)p.w;
+        double x = p.x, y = p.y, z = p.z;
+        if (pos64) {
+            const double4 q = pos64[i];
+            x = q.x;
+            y = q.y;
+            z = q.z;
+        }
+        const float4 w = vel4[i];
+        const double vx = w.x, vy = w.y, vz = w.z;
+        v[0] += m;
+        v[1] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+        v[2] += m * (double)u[i];
+        v[3] += 0.5 * m * (double)phi[i];
+        v[4] += m * vx;
+        v[5] += m * vy;
+        v[6] += m * vz;
+        v[7] += m * (y * vz - z * vy);
+        v[8] += m * (z * vx - x * vz);
+        v[9] += m * (x * vy - y * vx);
+    }
+#pragma unroll
+    for (int k = 0; k < kDiag; ++k) {
+        double x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < kDiag) {
+        double t = 0.0;
+        for (int w = 0; w < kDiagThreads / 32; ++w) t += red[threadIdx.x][w];
+        out[(size_t)blockIdx.x * kDiag + threadIdx.x] = t;
+    }
+}
+
+__global__ void k_diag_total(int blocks, double *partials, double *total) {
+    const int k = threadIdx.x;
+    if (k >= kDiag) return;
+    double t = 0.0;
+    for (int b = 0; b < blocks; ++b) t += partials[(size_t)b * kDiag + k];
+    total[k] = t;
 }
 
 // render.metal:49-66
@@ -623,7 +730,9 @@ size_t list_smem_opt_in() {
     cudaGetDevice(&dev);
     if (smem > 48 * 1024 && dev >= 0 && dev < 64 && !done[dev]) {
         cudaFuncSetAttribute(k_density<kLanesPerParticle>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_acceleration<kLanesPerParticle>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_acceleration<kLanesPerParticle, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        cudaFuncSetAttribute(k_acceleration<kLanesPerParticle, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
         done[dev] = true;
     }
@@ -682,7 +791,11 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     a.globals = ctx->globals;
     constexpr int parts = parts_per_block<kLanesPerParticle>();
     const size_t smem = list_smem_opt_in();
-    k_acceleration<kLanesPerParticle><<<(unsigned)((n + parts - 1) / parts), parts * kLanesPerParticle, smem, st>>>(a);
+    const unsigned blocks = (unsigned)((n + parts - 1) / parts);
+    if (ctx->form.precision == SPH_PRECISION_MIXED)
+        k_acceleration<kLanesPerParticle, true><<<blocks, parts * kLanesPerParticle, smem, st>>>(a);
+    else
+        k_acceleration<kLanesPerParticle, false><<<blocks, parts * kLanesPerParticle, smem, st>>>(a);
     return cuda_status(cudaGetLastError(), "acceleration");
 }
 
@@ -700,8 +813,28 @@ sph_status launch_step(sph_ctx *ctx, cudaStream_t st) {
     a.du = ctx->du;
     a.dhdt = ctx->dhdt;
     a.globals = ctx->globals;
-    k_step<<<(n + 255) / 256, 256, 0, st>>>(a);
+    a.pos64 = ctx->pos64;
+    a.dglob = ctx->dglob;
+    if (ctx->form.precision == SPH_PRECISION_MIXED)
+        k_step<true><<<(n + 255) / 256, 256, 0, st>>>(a);
+    else
+        k_step<false><<<(n + 255) / 256, 256, 0, st>>>(a);
     return cuda_status(cudaGetLastError(), "step");
+}
+
+sph_status launch_pos_to64(sph_ctx *ctx, cudaStream_t st) {
+    if (ctx->n > 0 && ctx->pos64) k_pos_to64<<<(ctx->n + 255) / 256, 256, 0, st>>>(ctx->n, ctx->pos4, ctx->pos64);
+    return cuda_status(cudaGetLastError(), "positions to FP64");
+}
+
+// ctx->diag: [kDiagBlocks * kDiag] partials, then kDiag totals
+sph_status launch_diag_sums(sph_ctx *ctx, cudaStream_t st) {
+    double *tot = ctx->diag + (size_t)kDiagBlocks * kDiag;
+    k_diag_block<<<kDiagBlocks, kDiagThreads, 0, st>>>(ctx->n, ctx->pos4,
+                                                       ctx->form.precision == SPH_PRECISION_MIXED ? ctx->pos64 : nullptr,
+                                                       ctx->vel4, ctx->u, ctx->phi, ctx->diag);
+    k_diag_total<<<1, 32, 0, st>>>(kDiagBlocks, ctx->diag, tot);
+    return cuda_status(cudaGetLastError(), "diagnostics");
 }
 
 sph_status launch_snapshot(sph_ctx *ctx, cudaStream_t st) {

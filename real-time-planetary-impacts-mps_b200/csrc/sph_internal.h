@@ -24,6 +24,12 @@
 
 namespace sph {
 
+// FP64 diagnostics sums: kDiag values (M, Ekin, Eint, Epot, P xyz, L xyz),
+// partials of kDiagBlocks blocks followed by the totals.
+constexpr int kDiag = 10;
+constexpr int kDiagBlocks = 148 * 4;
+constexpr int kDiagDoubles = (kDiagBlocks + 1) * kDiag;
+
 // One-sweep LSD radix sorter for (uint32 key, uint32 value) pairs.
 struct RadixSorter {
     uint32_t *keys[2] = {nullptr, nullptr};
@@ -96,6 +102,11 @@ struct sph_ctx {
     float *rho = nullptr, *u = nullptr, *P = nullptr, *h = nullptr, *f = nullptr, *c = nullptr;
     float *du = nullptr, *B = nullptr, *dhdt = nullptr, *gnorm = nullptr;
     float *phi = nullptr;  // potential (theta gravity form)
+    // mixed-precision form: FP64 master positions (x, y, z, -) and FP64 globals
+    // ([0] global time in seconds); the float positions are their roundings
+    double4 *pos64 = nullptr;
+    double *dglob = nullptr;
+    double *diag = nullptr;  // diagnostics: block partials, then the totals
     sph_form form{SPH_GRAVITY_REFERENCE, 0.5f, 0, 0};
     int32_t *mat = nullptr, *nat = nullptr;
     uint8_t *active = nullptr;
@@ -144,12 +155,19 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st);
 sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st);
 sph_status launch_step(sph_ctx *ctx, cudaStream_t st);
 sph_status launch_snapshot(sph_ctx *ctx, cudaStream_t st);
+// FP64 copies of the float positions (entering the mixed-precision form)
+sph_status launch_pos_to64(sph_ctx *ctx, cudaStream_t st);
+// FP64 conservation sums into ctx->diag (see sph_diagnostics)
+sph_status launch_diag_sums(sph_ctx *ctx, cudaStream_t st);
 
 // sph_gravity.cu
 sph_status launch_gravity(sph_ctx *ctx, cudaStream_t st);
 
 // sph_gravity_theta.cu
 sph_status launch_gravity_theta(sph_ctx *ctx, cudaStream_t st);
+// the potential alone (acceleration and |a| untouched), opening angle theta,
+// on the current GPU tree
+sph_status launch_potential_theta(sph_ctx *ctx, float theta, cudaStream_t st);
 sph_status launch_direct_f64(sph_ctx *ctx, const int32_t *d_targets, int nt, double *d_out, cudaStream_t st);
 
 // sph_tree.cu
