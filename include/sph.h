@@ -41,6 +41,7 @@ typedef enum {
 #define SPH_HEALTH_NAN_DENSITY       0x0008u /* a density or pressure came out non-finite */
 #define SPH_HEALTH_SCAN_TIMEOUT      0x0010u /* a scan look-back wait gave up */
 #define SPH_HEALTH_ROOT_LEAF         0x0020u /* the root is a leaf: gravity pass skipped */
+#define SPH_HEALTH_MLP_TIMEOUT       0x0040u /* a tensor-core wait of the h-seed network gave up */
 
 typedef struct sph_ctx sph_ctx;
 
@@ -154,13 +155,16 @@ sph_status sph_step(sph_ctx *ctx, void *stream);         /* Compute::stepPass (:
 #define SPH_PRECISION_REFERENCE 0 /* float positions drifted in float, as the reference (step.metal:45) */
 #define SPH_PRECISION_MIXED     1 /* FP64 master positions and global time (float working copies), Kahan-
                                      compensated acceleration, du/dt and dh/dt sums */
+#define SPH_HSEED_PLAIN   0 /* the iteration starts from the particle's own h (density.metal:73-74) */
+#define SPH_HSEED_LEARNED 1 /* it starts from the learned seed (sph_hseed_train), with fallback */
 typedef struct {
     int32_t gravity;   /* SPH_GRAVITY_* */
     float theta;       /* opening angle of SPH_GRAVITY_THETA: a node of radius r_node (about its centre of
                           mass) is accepted for a group of particles when r_node < theta d, d = the distance
                           from its centre of mass to the group's bounding box, and d > 2 x softening */
-    int32_t h_seed;    /* reserved, 0 */
+    int32_t h_seed;    /* SPH_HSEED_* */
     int32_t precision; /* SPH_PRECISION_* */
+    float h_tolerance; /* convergence test of the h iteration, |dh| / h <= tol; 0 = DENSITY_ETA (0.005) */
 } sph_form;
 void sph_form_default(sph_form *f); /* reference form, theta 0.5 */
 /* Select the form for the following passes (drops a captured step graph).
@@ -176,6 +180,43 @@ sph_status sph_get_form(const sph_ctx *ctx, sph_form *f);
  * gravity forms; no counterpart in the reference.  Synchronous. */
 sph_status sph_gravity_direct_f64(sph_ctx *ctx, const int32_t *targets, int32_t n_targets, double *out,
                                   void *stream);
+
+/* Learned smoothing-length seed (no counterpart in the reference).  An
+ * 8 -> 64 -> 64 -> 1 MLP, run and trained on the tensor cores (BF16 operands,
+ * FP32 accumulation), predicts from a particle's state at the start of the
+ * density pass the h its iteration converges to; SPH_HSEED_LEARNED starts the
+ * iteration there (density.metal:73-143), falling back to the plain guess
+ * when the first sweep moves the seed by more than 5%.
+ * sph_hseed_capture(ctx, 1): every following density pass records its
+ *   (features, converged h) pairs as the training set (the last pass's).
+ * sph_hseed_train: `iterations` Adam steps (learning rate lr) on minibatches
+ *   of `batch` rows drawn from the recorded set; the first call also fixes
+ *   the feature and target standardisation.  *loss = the last minibatch's
+ *   mean squared error (standardised target), may be NULL.  Synchronous.
+ * sph_hseed_gradient: the loss gradient of one minibatch (row r of the batch
+ *   is particle ((r * 0x9E3779B97F4A7C15) ^ salt) mod n, arithmetic modulo
+ *   2^64) without updating the weights: grads receives
+ *   sph_hseed_num_params() floats, in the order W1[64][8], b1[64],
+ *   W2[64][64], b2[64], w3[64], b3.  Synchronous.
+ * sph_hseed_params: copy the FP32 weights out (get) and/or in (set); either
+ *   may be NULL.  sph_hseed_dataset: the recorded raw features [n][8],
+ *   targets log(h_converged / h0) [n] and the standardisation (feature means
+ *   [8], feature 1/deviations [8], target mean, target deviation); any may be
+ *   NULL.
+ * sph_hseed_stats: counters of the last density pass. */
+typedef struct {
+    uint32_t sweeps;     /* density sweeps of the h iteration, summed over particles */
+    uint32_t fallbacks;  /* particles whose learned seed was abandoned */
+    uint32_t max_sweeps; /* most sweeps of one particle */
+    uint32_t particles;  /* particles iterated */
+} sph_hseed_stats;
+int32_t sph_hseed_num_params(void);
+sph_status sph_hseed_capture(sph_ctx *ctx, int32_t on);
+sph_status sph_hseed_train(sph_ctx *ctx, int32_t iterations, int32_t batch, float lr, float *loss, void *stream);
+sph_status sph_hseed_gradient(sph_ctx *ctx, int32_t batch, uint32_t salt, float *grads, float *loss, void *stream);
+sph_status sph_hseed_params(sph_ctx *ctx, float *get, const float *set);
+sph_status sph_hseed_dataset(sph_ctx *ctx, float *features, float *targets, float *norm);
+sph_status sph_hseed_get_stats(sph_ctx *ctx, sph_hseed_stats *out);
 
 /* FP64 conservation diagnostics (no counterpart in the reference, which
  * computes no potential: L2P.metal:12-32 returns only the acceleration).

@@ -18,8 +18,9 @@ LIB_PATH = os.path.join(HERE, "libsph_b200.so")
 # sequential order.  Only the parity tests load it; it is not the product.
 PARITY_LIB_PATH = os.path.join(HERE, "libsph_b200_parity.so")
 PARITY_FLAGS = ["-fmad=false", "-DSPH_PARITY"]
-SOURCES = ["sph_api.cu", "sph_sort.cu", "sph_hydro.cu", "sph_gravity.cu", "sph_gravity_theta.cu", "sph_tree.cu"]
-HEADERS = ["sph_common.cuh", "sph_internal.h"]
+SOURCES = ["sph_api.cu", "sph_sort.cu", "sph_hydro.cu", "sph_gravity.cu", "sph_gravity_theta.cu", "sph_tree.cu",
+           "sph_hseed.cu"]
+HEADERS = ["sph_common.cuh", "sph_internal.h", "sph_tc.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared"]
 
@@ -42,7 +43,7 @@ FIELDS = {
 VECTOR_FIELDS = ("pos", "vel", "acc")
 
 HEALTH = {"sort_timeout": 0x1, "list_capacity": 0x2, "tree_capacity": 0x4, "nan_density": 0x8,
-          "scan_timeout": 0x10, "root_leaf": 0x20}
+          "scan_timeout": 0x10, "root_leaf": 0x20, "mlp_timeout": 0x40}
 
 
 class SphParams(C.Structure):
@@ -70,7 +71,17 @@ class SphIC(C.Structure):
 
 
 class SphForm(C.Structure):
-    _fields_ = [("gravity", C.c_int32), ("theta", C.c_float), ("h_seed", C.c_int32), ("precision", C.c_int32)]
+    _fields_ = [("gravity", C.c_int32), ("theta", C.c_float), ("h_seed", C.c_int32), ("precision", C.c_int32),
+                ("h_tolerance", C.c_float)]
+
+
+class SphHSeedStats(C.Structure):
+    _fields_ = [("sweeps", C.c_uint32), ("fallbacks", C.c_uint32), ("max_sweeps", C.c_uint32),
+                ("particles", C.c_uint32)]
+
+
+SPH_HSEED_PLAIN = 0
+SPH_HSEED_LEARNED = 1
 
 
 SPH_PRECISION_REFERENCE = 0
@@ -172,6 +183,13 @@ def load(parity: bool = False) -> C.CDLL:
         "sph_get_form": (st, [vp, C.POINTER(SphForm)]),
         "sph_gravity_direct_f64": (st, [vp, _ip, C.c_int32, C.POINTER(C.c_double), vp]),
         "sph_diagnostics": (st, [vp, vp, C.c_float, C.POINTER(SphDiag)]),
+        "sph_hseed_num_params": (C.c_int32, []),
+        "sph_hseed_capture": (st, [vp, C.c_int32]),
+        "sph_hseed_train": (st, [vp, C.c_int32, C.c_int32, C.c_float, _fp, vp]),
+        "sph_hseed_gradient": (st, [vp, C.c_int32, C.c_uint32, _fp, _fp, vp]),
+        "sph_hseed_params": (st, [vp, _fp, _fp]),
+        "sph_hseed_dataset": (st, [vp, _fp, _fp, _fp]),
+        "sph_hseed_get_stats": (st, [vp, C.POINTER(SphHSeedStats)]),
         "sph_draw_snapshot": (st, [vp, vp, _ip]),
         "sph_upload": (st, [vp, C.c_int, vp, C.c_size_t]),
         "sph_download": (st, [vp, C.c_int, vp, C.c_size_t]),

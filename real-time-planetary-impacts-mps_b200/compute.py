@@ -176,23 +176,74 @@ class Compute:
                     n_levels=nl.value, n_nodes=nn.value)
 
     # ---- numerical forms (no reference counterpart) --------------------
-    def set_form(self, gravity: str = "reference", theta: float = 0.5, precision: str = "reference"):
+    def set_form(self, gravity: str = "reference", theta: float = 0.5, precision: str = "reference",
+                 h_seed: str = "plain", h_tolerance: float = 0.0):
         """Select the numerical form: gravity "reference" (the reference's
         logic) or "theta" (opening-angle group walk with exact near field);
         precision "reference" (float positions) or "mixed" (FP64 master
-        positions and time, Kahan-compensated sums)."""
+        positions and time, Kahan-compensated sums); h_seed "plain" or
+        "learned" (the trained MLP starts the density iteration);
+        h_tolerance of the density iteration (0 = the reference's 0.005)."""
         f = _lib.SphForm()
         self._lib.sph_form_default(C.byref(f))
         f.gravity = _lib.SPH_GRAVITY_THETA if gravity == "theta" else _lib.SPH_GRAVITY_REFERENCE
         f.theta = float(theta)
         f.precision = _lib.SPH_PRECISION_MIXED if precision == "mixed" else _lib.SPH_PRECISION_REFERENCE
+        f.h_seed = _lib.SPH_HSEED_LEARNED if h_seed == "learned" else _lib.SPH_HSEED_PLAIN
+        f.h_tolerance = float(h_tolerance)
         self._check(self._lib.sph_set_form(self._h, C.byref(f)), "sph_set_form")
 
     def get_form(self) -> dict:
         f = _lib.SphForm()
         self._check(self._lib.sph_get_form(self._h, C.byref(f)), "sph_get_form")
         return dict(gravity="theta" if f.gravity == _lib.SPH_GRAVITY_THETA else "reference", theta=f.theta,
-                    precision="mixed" if f.precision == _lib.SPH_PRECISION_MIXED else "reference")
+                    precision="mixed" if f.precision == _lib.SPH_PRECISION_MIXED else "reference",
+                    h_seed="learned" if f.h_seed == _lib.SPH_HSEED_LEARNED else "plain", h_tolerance=f.h_tolerance)
+
+    # ---- learned smoothing-length seed (no reference counterpart) ------
+    def hseed_capture(self, on: bool = True):
+        """Record (features, converged h) of every following density pass."""
+        self._check(self._lib.sph_hseed_capture(self._h, 1 if on else 0), "sph_hseed_capture")
+
+    def hseed_train(self, iterations: int, batch: int = 16384, lr: float = 1e-3, stream=None) -> float:
+        """Adam steps on the recorded pass; returns the last minibatch loss."""
+        loss = C.c_float()
+        self._check(self._lib.sph_hseed_train(self._h, int(iterations), int(batch), float(lr), C.byref(loss),
+                                              _stream(stream)), "sph_hseed_train")
+        return loss.value
+
+    def hseed_gradient(self, batch: int, salt: int, stream=None):
+        """(gradient, loss) of one minibatch, weights unchanged."""
+        g = np.zeros(self._lib.sph_hseed_num_params(), np.float32)
+        loss = C.c_float()
+        self._check(self._lib.sph_hseed_gradient(self._h, int(batch), int(salt) & 0xFFFFFFFF, _ptr(g, _fp),
+                                                 C.byref(loss), _stream(stream)), "sph_hseed_gradient")
+        return g, loss.value
+
+    def hseed_params(self, set_to=None) -> np.ndarray:
+        """The FP32 weights (after setting them to `set_to` when given)."""
+        if set_to is not None:
+            w = np.ascontiguousarray(np.asarray(set_to, np.float32))
+            self._check(self._lib.sph_hseed_params(self._h, None, _ptr(w, _fp)), "sph_hseed_params")
+        out = np.zeros(self._lib.sph_hseed_num_params(), np.float32)
+        self._check(self._lib.sph_hseed_params(self._h, _ptr(out, _fp), None), "sph_hseed_params")
+        return out
+
+    def hseed_dataset(self):
+        """(features [n, 8], targets [n], standardisation [18]) of the recorded pass."""
+        n = self.nParticles
+        X = np.zeros((n, 8), np.float32)
+        y = np.zeros(n, np.float32)
+        norm = np.zeros(18, np.float32)
+        self._check(self._lib.sph_hseed_dataset(self._h, _ptr(X, _fp), _ptr(y, _fp), _ptr(norm, _fp)),
+                    "sph_hseed_dataset")
+        return X, y, norm
+
+    def hseed_stats(self) -> dict:
+        """Counters of the last density pass's h iteration."""
+        st = _lib.SphHSeedStats()
+        self._check(self._lib.sph_hseed_get_stats(self._h, C.byref(st)), "sph_hseed_get_stats")
+        return dict(sweeps=st.sweeps, fallbacks=st.fallbacks, max_sweeps=st.max_sweeps, particles=st.particles)
 
     def diagnostics(self, stream=None, theta_potential: float = 0.5) -> dict:
         """FP64 conservation sums (mass, energies, momentum, angular momentum)."""

@@ -277,6 +277,7 @@ sph_status sph_destroy(sph_ctx *ctx) {
                     ctx->diag};
     for (void *b : bufs) cudaFree(b);
     sort_free(ctx->cell_sort);
+    hseed_free(ctx);
     tree_free(ctx);
     tree_storage_free(ctx->tree);
     delete ctx;
@@ -798,8 +799,9 @@ void sph_form_default(sph_form *f) {
     if (!f) return;
     f->gravity = SPH_GRAVITY_REFERENCE;
     f->theta = 0.5f;
-    f->h_seed = 0;
-    f->precision = 0;
+    f->h_seed = SPH_HSEED_PLAIN;
+    f->precision = SPH_PRECISION_REFERENCE;
+    f->h_tolerance = 0.f;
 }
 
 sph_status sph_set_form(sph_ctx *ctx, const sph_form *f) {
@@ -812,9 +814,17 @@ sph_status sph_set_form(sph_ctx *ctx, const sph_form *f) {
         set_error("sph_set_form: theta = %g is outside (0, 1.5]", (double)f->theta);
         return SPH_ERR_INVALID_ARG;
     }
-    if (f->h_seed != 0) {
-        set_error("sph_set_form: h_seed must be 0");
-        return SPH_ERR_UNSUPPORTED;
+    if (f->h_seed != SPH_HSEED_PLAIN && f->h_seed != SPH_HSEED_LEARNED) {
+        set_error("sph_set_form: h_seed = %d is not a SPH_HSEED_* value", (int)f->h_seed);
+        return SPH_ERR_INVALID_ARG;
+    }
+    if (f->h_seed == SPH_HSEED_LEARNED && !ctx->hs.have_norm) {
+        set_error("sph_set_form: the learned h seed is not trained yet (sph_hseed_train)");
+        return SPH_ERR_INVALID_ARG;
+    }
+    if (!(f->h_tolerance >= 0.f && f->h_tolerance < 1.f)) {
+        set_error("sph_set_form: h_tolerance = %g is outside [0, 1)", (double)f->h_tolerance);
+        return SPH_ERR_INVALID_ARG;
     }
     if (f->precision != SPH_PRECISION_REFERENCE && f->precision != SPH_PRECISION_MIXED) {
         set_error("sph_set_form: precision = %d is not a SPH_PRECISION_* value", (int)f->precision);

@@ -237,7 +237,15 @@ struct DensityArgs {
     int32_t *globals;
     uint32_t *health;
     EosTables eos;
+    float eta;            // convergence tolerance of the h iteration (DENSITY_ETA in the reference)
+    const float *seed;    // learned starting h per particle, or null (the plain guess, h itself)
+    float *nn_out;        // neighbour count per particle, or null
+    uint32_t *stats;      // [0] sweeps, [1] fallbacks, [2] most sweeps, [3] particles; or null
 };
+
+// A learned seed whose first sweep moves h by more than this relative amount
+// is abandoned for the plain initial guess.
+constexpr float kSeedFallback = 0.05f;
 
 // Per-particle neighbour list of the density pass, in shared memory: the
 // sorted indices of every candidate within kListReach x the smoothing length
@@ -283,7 +291,20 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArg
         return;
     }
     const float px = me.x, py = me.y, pz = me.z, mi = me.w;
-    float hi = a.h[ind];
+    const float h_plain = a.h[ind];
+    float hi = h_plain;
+    // a learned seed replaces the plain guess when it is finite and within a
+    // factor two of it
+    bool seeded = false;
+    if (a.seed) {
+        const float sd = a.seed[ind];
+        if (sd >= 0.5f * h_plain && sd <= 2.f * h_plain && sd <= kMaxH) {
+            hi = sd;
+            seeded = true;
+        }
+    }
+    bool first = true, fell_back = false;
+    int sweeps = 0;
     int max_h = 0;  // an int in the reference (truncates h < 1 to 0)
     float h2x4 = 4.f * hi * hi;
     float h1 = 1.f / hi;
@@ -314,7 +335,7 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArg
             [](int) { return false; });
         __syncwarp(gm);
     };
-    while (eps > kDensityEta && count < kMaxNR) {
+    while (eps > a.eta && count < kMaxNR) {
         const bool cached = hi < (float)max_h && nn < kNeighbourCache;
         if (!cached) {
             hs = hi;
@@ -352,7 +373,22 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArg
         float nh = fmin_ref(kResolutionEta * powf(mi / dens, 1.f / 3), kMaxH);
         nh = 0.5f * (hi + nh);
         eps = fabsf(nh - hi) / hi;
-        if (eps > kDensityEta) {
+        ++sweeps;
+        if (first && seeded && eps > kSeedFallback) {
+            // the seed disagrees with its own first sweep: start again from
+            // the plain guess, with the iteration state of a fresh start
+            first = false;
+            fell_back = true;
+            hi = h_plain;
+            h1 = 1.f / hi;
+            h2x4 = 4.f * hi * hi;
+            max_h = 0;
+            nn = 0;
+            eps = 1.f;
+            continue;
+        }
+        first = false;
+        if (eps > a.eta) {
             max_h = (int)fmax_ref((float)max_h, hi);
             hi = nh;
             h1 = 1.f / hi;
@@ -414,7 +450,23 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArg
     cx = group_sum<L>(cx, gm);
     cy = group_sum<L>(cy, gm);
     cz = group_sum<L>(cz, gm);
+    if (a.stats) {
+        // counters of the iteration (one group member per particle)
+        const unsigned am = __activemask();
+        const uint32_t mine = sub == 0 ? 1u : 0u;
+        const uint32_t sw = __reduce_add_sync(am, mine * (uint32_t)sweeps);
+        const uint32_t fb = __reduce_add_sync(am, mine * (fell_back ? 1u : 0u));
+        const uint32_t mx = __reduce_max_sync(am, mine * (uint32_t)sweeps);
+        const uint32_t np = __reduce_add_sync(am, mine);
+        if ((threadIdx.x & 31) == (uint32_t)(__ffs(am) - 1)) {
+            atomicAdd(a.stats + 0, sw);
+            if (fb) atomicAdd(a.stats + 1, fb);
+            atomicMax(a.stats + 2, mx);
+            atomicAdd(a.stats + 3, np);
+        }
+    }
     if (sub != 0) return;
+    if (a.nn_out) a.nn_out[ind] = (float)nn;
     vdiv = fabsf(vdiv) / dens;
     float acurl = sqrtf(cx * cx + cy * cy + cz * cz) / dens;
     float fi = 1.f / (1.f + (hi / (3.f * dens)) * dens_h);
@@ -767,9 +819,25 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     a.globals = ctx->globals;
     a.health = ctx->health;
     a.eos = ctx->eos;
+    a.eta = ctx->form.h_tolerance > 0.f ? ctx->form.h_tolerance : kDensityEta;
+    a.seed = nullptr;
+    a.nn_out = ctx->hs.nn;
+    a.stats = ctx->hs.stats;
+    sph_status s = SPH_OK;
+    if (ctx->hs.stats) cudaMemsetAsync(ctx->hs.stats, 0, sizeof(uint32_t) * 4, st);
+    if (ctx->hs.capture) s = launch_hseed_capture(ctx, st);
+    if (s == SPH_OK && ctx->form.h_seed == SPH_HSEED_LEARNED) {
+        s = launch_hseed_infer(ctx, st);
+        a.seed = ctx->hs.seed;
+    }
+    if (s != SPH_OK) return s;
+    a.nn_out = ctx->hs.nn;
+    a.stats = ctx->hs.stats;
     constexpr int parts = parts_per_block<kLanesPerParticle>();
     const size_t smem = list_smem_opt_in();
     k_density<kLanesPerParticle><<<(unsigned)((n + parts - 1) / parts), parts * kLanesPerParticle, smem, st>>>(a);
+    if (ctx->hs.capture) s = launch_hseed_targets(ctx, st);
+    if (s != SPH_OK) return s;
     return cuda_status(cudaGetLastError(), "density");
 }
 

@@ -90,6 +90,39 @@ struct TreeBuild {
     int64_t walk_queue_ints = 0;
 };
 
+// Learned smoothing-length seed (sph_hseed.cu): FP32 master weights and Adam
+// state, the feature normalisation, the captured training set and the seed.
+struct HSeed {
+    float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    float *norm = nullptr;
+    double *norm_part = nullptr;
+    float *X = nullptr;     // [n][8] raw features of the captured pass
+    float *y = nullptr;     // [n] targets log(h_converged / h0)
+    float *h0 = nullptr;    // [n] h at the start of the captured pass
+    float *nn = nullptr;    // [n] neighbour count of the last density pass
+    float *seed = nullptr;  // [n] predicted starting h
+    float *loss = nullptr;  // running loss of a training call
+    uint32_t *stats = nullptr;  // density-pass counters: [0] NR iterations, [1] fallbacks, [2] max, [3] particles
+    int steps = 0;          // Adam steps taken
+    bool have_data = false, have_norm = false, capture = false;
+};
+
+struct HSeedArgs {
+    int n;
+    const float *h, *dhdt, *rho, *u;
+    const int32_t *mat, *nat;
+    const uint8_t *active;
+    const int32_t *globals;
+    const float *nn;
+    float *X, *y, *h0, *seed;
+    const float *params;
+    float *grads;
+    const float *norm;
+    float *loss;
+    uint32_t *health;
+    uint32_t salt;
+};
+
 }  // namespace sph
 
 struct sph_ctx {
@@ -107,7 +140,7 @@ struct sph_ctx {
     double4 *pos64 = nullptr;
     double *dglob = nullptr;
     double *diag = nullptr;  // diagnostics: block partials, then the totals
-    sph_form form{SPH_GRAVITY_REFERENCE, 0.5f, 0, 0};
+    sph_form form{SPH_GRAVITY_REFERENCE, 0.5f, SPH_HSEED_PLAIN, SPH_PRECISION_REFERENCE, 0.f};
     int32_t *mat = nullptr, *nat = nullptr;
     uint8_t *active = nullptr;
     int32_t *globals = nullptr;
@@ -128,6 +161,8 @@ struct sph_ctx {
     void *stage = nullptr;  // device staging for uploads/downloads
     size_t stage_bytes = 0;
     int32_t *snapshot = nullptr;
+
+    sph::HSeed hs;
 
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
@@ -162,6 +197,18 @@ sph_status launch_diag_sums(sph_ctx *ctx, cudaStream_t st);
 
 // sph_gravity.cu
 sph_status launch_gravity(sph_ctx *ctx, cudaStream_t st);
+
+// sph_hseed.cu
+sph_status hseed_alloc(sph_ctx *ctx);
+void hseed_free(sph_ctx *ctx);
+int hseed_num_params();
+int hseed_norm_size();
+sph_status launch_hseed_capture(sph_ctx *ctx, cudaStream_t st);
+sph_status launch_hseed_targets(sph_ctx *ctx, cudaStream_t st);
+sph_status launch_hseed_infer(sph_ctx *ctx, cudaStream_t st);
+sph_status launch_hseed_norm(sph_ctx *ctx, cudaStream_t st);
+sph_status launch_hseed_grad(sph_ctx *ctx, uint32_t it, int batch, uint32_t salt, cudaStream_t st);
+sph_status launch_hseed_adam(sph_ctx *ctx, float lr, cudaStream_t st);
 
 // sph_gravity_theta.cu
 sph_status launch_gravity_theta(sph_ctx *ctx, cudaStream_t st);
