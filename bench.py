@@ -1,12 +1,25 @@
 #!/usr/bin/env python
-"""Benchmark: particle-steps/s of the full SPH + FMM step at N = 1e6 on B200.
+"""Benchmark: particle-steps/s of the full SPH + FMM step at N = 1e6 on B200,
+the chosen form against the plain form.
 
-One step = GPU octree build, sort (hash, radix sort, cell ranges), gravity
-(up pass, down pass, L2P + P2P), density, acceleration, kick/drift -- the
-reference's Headless::step without the snapshot -- on a seeded two-body impact
-of 800k + 200k particles (the 16384 + 4096 generator rescaled), leaf capacity
-32, depth 7.  The state (~150 B/particle plus the 128 MiB cell table) is larger
-than the 126 MB L2, so no flush is needed between steps.
+One step = GPU octree build, sort (hash, radix sort, cell ranges), gravity,
+density, acceleration, kick/drift -- the reference's Headless::step without
+the snapshot -- on a seeded two-body impact of 800k + 200k particles (the
+16384 + 4096 generator rescaled), leaf capacity 32, depth 7.  The state
+(~150 B/particle plus the 128 MiB cell table) is larger than the 126 MB L2,
+so no flush is needed between steps.
+
+Forms (one context each, same initial conditions):
+  plain   the reference's logic (its adaptive gravity acceptance, float
+          positions, plain initial h guess) -- what the parity tests pin;
+  chosen  opening-angle gravity (theta, default 0.6), mixed precision (FP64
+          master positions and time, Kahan sums) and the learned h seed,
+          trained online on the first steps' density passes.
+`value` is the chosen form; `chosen_over_plain` is the ratio of the two
+graph-replayed step times.  The line also carries the gravity error of both
+forms against an FP64 direct sum (16 384 targets), the total-energy drift of
+both over `--drift-steps` further steps, and the learned seed's iteration
+counts.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -18,6 +31,7 @@ exchange), launched by torchrun; value = all ranks' particle-steps / max time.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import importlib
 import json
 import os
@@ -40,19 +54,21 @@ ALGO_BYTES = {"tree": 76, "sort": 92, "gravity": 44, "density": 65, "acceleratio
 PASS_KERNELS = {
     "tree": "k_bbox, k_tree_keys, k_onesweep x3, k_children/k_emit/scan x7, k_marks, k_write, k_link",
     "sort": "k_hash_hist, k_onesweep x3, k_cells",
-    "gravity": "k_up x8, k_down x8",
-    "density": "k_gather, k_density",
+    "gravity": "plain: k_up x8, k_down x8; chosen: k_up_theta x8, k_gather_key_order, k_walk",
+    "density": "k_gather, [k_mlp (learned seed)], k_density",
     "acceleration": "k_acceleration",
     "step": "k_step",
 }
-LAUNCHES_PER_STEP = None  # filled from the pass structure below
 
 
-def launches_per_step(depth: int) -> int:
-    tree = 1 + 1 + 1 + 3 + 1 + depth * (1 + 4 + 1) + 1 + 1 + (depth + 1) + 4 + 4 + (depth + 1) + depth
+def launches_per_step(depth: int, chosen: bool) -> int:
+    """Kernels of one step (memsets excluded), counted from the pass structure."""
+    scan = 4  # reduce, blocks, apply, total
+    tree = 3 + 3 + 1 + depth * (1 + scan + 1) + 1 + 1 + (depth + 1) + 2 * scan + (depth + 1) + depth
     sort = 1 + 3 + 1
-    gravity = 2 * (depth + 1)
-    return tree + sort + gravity + 2 + 1 + 1
+    gravity = (depth + 1) + 2 if chosen else 2 * (depth + 1)
+    density = 2 + (1 if chosen else 0)
+    return tree + sort + gravity + density + 1 + 1
 
 
 def load_peaks() -> dict:
@@ -62,6 +78,15 @@ def load_peaks() -> dict:
         return {"hbm_gbs": float(p["hbm_gbs"]), "source": "measured"}
     except Exception:
         return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def load_traffic() -> dict:
+    """DRAM bytes per launch of the kernels captured with ncu (profiles/)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
 
 
 class ClockSampler:
@@ -129,9 +154,24 @@ def make_ic(seed: int, scale: float = 1.0):
     return ic_mod.make_impact(int(N_TARGET * scale), int(N_IMPACTOR * scale), seed=seed)
 
 
-def cpu_reference(ic: dict, steps: int, warmup: int, budget_s: float | None = None) -> dict:
+def host_cores() -> dict:
+    """Logical CPUs usable here and the physical core count (lscpu)."""
+    logical = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    physical = None
+    try:
+        out = subprocess.run(["lscpu", "-p=CORE,SOCKET"], capture_output=True, text=True, timeout=10).stdout
+        cores = {tuple(l.split(",")) for l in out.splitlines() if l and not l.startswith("#")}
+        physical = len(cores) or None
+    except Exception:
+        pass
+    return {"logical": logical, "physical": physical}
+
+
+def cpu_reference(ic: dict, steps: int, warmup: int, budget_s: float | None = None, threads: int | None = None) -> dict:
     """The reference's kernels on the host cores (oracle/_ref when built, else
     the oracle restatement), full N, reference CPU octree rebuilt every step."""
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O  # noqa: E402 -- CPU-baseline leg only
     eos_mod = importlib.import_module("real-time-planetary-impacts-mps_b200.eos_tables")
@@ -142,7 +182,7 @@ def cpu_reference(ic: dict, steps: int, warmup: int, budget_s: float | None = No
     ef = O.aneos_load(tabs["forsterite"], 2048)
     ee = O.aneos_load(tabs["Fe85Si15"], 2048)
     st = O.OracleState(ic, ef, ee, kind=kind)
-    cores = O.load("oracle").ora_get_threads() if kind == "oracle" else (os.cpu_count() or 1)
+    hc = host_cores()
 
     def tree_fn(p):
         return O.tree_reference(p, LEAF, DEPTH, kind=kind)
@@ -157,10 +197,12 @@ def cpu_reference(ic: dict, steps: int, warmup: int, budget_s: float | None = No
         if budget_s is not None and time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    return {"value": st.n * done / dt, "unit": "particle-steps/s", "cores": cores,
+    used = int(os.environ.get("OMP_NUM_THREADS", hc["logical"]))
+    return {"value": st.n * done / dt, "unit": "particle-steps/s", "cores": used,
+            "physical_cores": hc["physical"], "logical_cpus": hc["logical"],
             "kind": "reference" if kind == "ref" else "port", "steps": done, "seconds": dt,
             "sample": f"{done} full step(s) of the N={st.n} impact after {warmup} warm-up step(s), "
-                      f"reference CPU octree (leaf {LEAF}) rebuilt each step, all passes"}
+                      f"reference CPU octree (leaf {LEAF}) rebuilt each step, all passes, {used} threads"}
 
 
 def run_reference_arm(args, rank: int, world: int):
@@ -173,11 +215,106 @@ def run_reference_arm(args, rank: int, world: int):
             "ms_per_step": 1e3 * cb["seconds"] / max(cb["steps"], 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"two-body impact N={ic['n']} (800k+200k), leaf {LEAF}, depth {DEPTH}, "
-                                   "plain form", "n_particles": int(ic["n"]), "parallelism": "replicas"},
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                                   "the reference's logic", "n_particles": int(ic["n"]), "parallelism": "replicas"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "physical_cores")},
             "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def graph_time(c, stream, K: int) -> tuple[float, str]:
+    """Device time (ms) of K full steps captured into one CUDA graph."""
+    import torch
+    calls = (c.updateOctreeBuffer, c.sort, c.gravitationalPass, c.densityPass, c.accelerationPass, c.stepPass)
+    try:
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            for _ in range(K):
+                for f in calls:
+                    f(stream)
+        mode = "cuda-graph"
+    except Exception as exc:
+        graph, mode = None, f"eager ({type(exc).__name__})"
+    stream.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    with torch.cuda.stream(stream):
+        if graph is not None:
+            graph.replay()
+        else:
+            for _ in range(K):
+                for f in calls:
+                    f(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    c.synchronize()
+    del graph
+    return t0.elapsed_time(t1), mode
+
+
+def pass_times(c, stream, K: int) -> dict:
+    """Per-pass device times (ms), eager with events between the passes."""
+    import torch
+    calls = (c.updateOctreeBuffer, c.sort, c.gravitationalPass, c.densityPass, c.accelerationPass, c.stepPass)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(PASSES) + 1)] for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            ev[k][0].record(stream)
+            for j, f in enumerate(calls):
+                f(stream)
+                ev[k][j + 1].record(stream)
+    torch.cuda.synchronize()
+    c.synchronize()
+    return {p: sum(ev[k][j].elapsed_time(ev[k][j + 1]) for k in range(K)) / K for j, p in enumerate(PASSES)}
+
+
+def gravity_error(c, targets) -> dict:
+    """Median / p99 relative acceleration error of the form's gravity pass
+    against the FP64 direct sum, at the current positions."""
+    ref = c.gravity_direct_f64(targets)
+    c.updateOctreeBuffer()
+    c.sort()
+    c.gravitationalPass()
+    c.synchronize()
+    a = c.download("acc")[targets].astype(np.float64)
+    e = np.linalg.norm(a - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+    return {"median": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
+            "targets": int(targets.size), "reference": "FP64 direct sum, cubic-spline softening 0.04"}
+
+
+def energy_drift(c, steps: int, chunk: int = 100) -> dict:
+    log("  drift: first diagnostics")
+    d0 = c.diagnostics()
+    worst, done = 0.0, 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        c.step_all(k)
+        done += k
+        d = c.diagnostics()
+        worst = max(worst, abs(d["total"] - d0["total"]) / abs(d0["total"]))
+        log(f"  drift: {done} steps, |dE|/|E0| so far {worst:.3e}")
+    c.synchronize()
+    return {"steps": steps, "max_rel_change_total_energy": worst, "e0": d0["total"],
+            "sampled_every": chunk}
+
+
+def fp32_peak(lib, stream) -> float:
+    """Measured FP32 FMA throughput (TFLOP/s) of this device."""
+    import torch
+    blocks, iters = 148 * 16, 8192
+    sink = torch.zeros(blocks, dtype=torch.float32, device="cuda")
+    s = ctypes.c_void_p(stream.cuda_stream)
+    for _ in range(2):
+        lib.sph_probe_fp32_fma(blocks, iters, ctypes.c_void_p(sink.data_ptr()), s)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(5):
+        lib.sph_probe_fp32_fma(blocks, iters, ctypes.c_void_p(sink.data_ptr()), s)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    flops = 5.0 * blocks * 256 * iters * 16
+    return flops / (t0.elapsed_time(t1) / 1e3) / 1e12
 
 
 def main():
@@ -189,6 +326,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="particle count relative to 1e6 (diagnostics)")
+    ap.add_argument("--theta", type=float, default=0.6, help="opening angle of the chosen form's gravity")
+    ap.add_argument("--train-iters", type=int, default=150, help="Adam steps after each warm-up step")
+    ap.add_argument("--drift-steps", type=int, default=100,
+                    help="steps of the energy-drift comparison (the 1000-step comparison runs at config 0 in the tests)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -208,34 +349,41 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     ic = make_ic(rank, args.scale)
-    log(f"ic ready: {ic['n']} particles")
     n = int(ic["n"])
-    c = pkg.Compute(ic, max_children_in_leaf=LEAF, max_tree_depth=DEPTH)
+    log(f"ic ready: {n} particles")
     stream = torch.cuda.Stream()
-    # warm-up: the first steps carry the reference's cold-start gravity (no |a| yet)
+    lib = pkg._lib.load()
+    peak32 = fp32_peak(lib, stream)
+    log(f"fp32 fma peak {peak32:.1f} TFLOP/s")
+    K = args.steps
+
+    # ---- plain form -------------------------------------------------------
+    cp = pkg.Compute(ic, max_children_in_leaf=LEAF, max_tree_depth=DEPTH)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            c.step(stream)
+            cp.step(stream)
+    stream.synchronize()
+    cp.synchronize()
+    # ---- chosen form: theta gravity, mixed precision, learned h seed --------
+    cc = pkg.Compute(ic, max_children_in_leaf=LEAF, max_tree_depth=DEPTH)
+    cc.set_form(gravity="theta", theta=args.theta, precision="mixed")
+    cc.hseed_capture(True)
+    train_ms = []
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            cc.step(stream)
             stream.synchronize()
-            log("warm-up step done")
+            t0 = time.perf_counter()
+            cc.hseed_train(args.train_iters, 16384, 1e-3, stream)
+            train_ms.append((time.perf_counter() - t0) * 1e3)
+    cc.hseed_capture(False)
+    cc.set_form(gravity="theta", theta=args.theta, precision="mixed", h_seed="learned")
+    with torch.cuda.stream(stream):
+        cc.step(stream)
     stream.synchronize()
-    c.synchronize()
+    cc.synchronize()
+    log(f"warm-up done; seed training {np.mean(train_ms):.1f} ms per call of {args.train_iters} Adam steps")
 
-    # the timed region replays K full steps captured into one CUDA graph
-    K = args.steps
-    calls = (c.updateOctreeBuffer, c.sort, c.gravitationalPass, c.densityPass, c.accelerationPass, c.stepPass)
-    graph = None
-    try:
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph, stream=stream):
-            for k in range(K):
-                for f in calls:
-                    f(stream)
-        mode = "cuda-graph"
-    except Exception as exc:  # eager launches instead
-        graph = None
-        mode = f"eager ({type(exc).__name__})"
-    stream.synchronize()
     uuid = None
     try:
         uuid = str(torch.cuda.get_device_properties(local).uuid)
@@ -244,106 +392,120 @@ def main():
     except Exception:
         uuid = None
     sampler = ClockSampler(uuid)
-    log(f"timing mode {mode}")
     sampler.start()
     time.sleep(0.3)
     if dist is not None:
         dist.barrier()
-    torch.cuda.synchronize()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    if graph is not None:
-        with torch.cuda.stream(stream):  # replay() launches on the current stream
-            graph.replay()
-    else:
-        with torch.cuda.stream(stream):
-            for k in range(K):
-                for f in calls:
-                    f(stream)
-    t_end.record(stream)
-    torch.cuda.synchronize()
+    plain_ms, mode = graph_time(cp, stream, K)
+    chosen_ms, mode_c = graph_time(cc, stream, K)
     if dist is not None:
         dist.barrier()
     clocks = sampler.stop()
-    c.synchronize()
-    elapsed_ms = t_start.elapsed_time(t_end)
     if dist is not None:
-        t = torch.tensor([elapsed_ms], device="cuda")
+        t = torch.tensor([plain_ms, chosen_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
-    value = world * n * K / (elapsed_ms / 1e3)
-    log(f"timed region: {elapsed_ms / K:.3f} ms/step")
+        plain_ms, chosen_ms = float(t[0]), float(t[1])
+    value = world * n * K / (chosen_ms / 1e3)
+    plain_value = world * n * K / (plain_ms / 1e3)
+    log(f"timed: plain {plain_ms / K:.3f} ms/step, chosen {chosen_ms / K:.3f} ms/step")
 
-    # per-pass split: K more steps, eager, with an event between passes on the
-    # launching stream (events inside a captured graph cannot be timed)
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(PASSES) + 1)] for _ in range(K)]
-    with torch.cuda.stream(stream):
-        for k in range(K):
-            ev[k][0].record(stream)
-            for j, f in enumerate(calls):
-                f(stream)
-                ev[k][j + 1].record(stream)
-    torch.cuda.synchronize()
-    c.synchronize()
-    per_pass = {p: 0.0 for p in PASSES}
-    for k in range(K):
-        for j, p in enumerate(PASSES):
-            per_pass[p] += ev[k][j].elapsed_time(ev[k][j + 1])
-    per_pass = {p: v / K for p, v in per_pass.items()}
-    log("per-pass ms: " + ", ".join(f"{p} {v:.3f}" for p, v in per_pass.items()))
+    pp = pass_times(cp, stream, K)
+    pc = pass_times(cc, stream, K)
+    st = cc.hseed_stats()
+    log("plain  per-pass ms: " + ", ".join(f"{p} {v:.3f}" for p, v in pp.items()))
+    log("chosen per-pass ms: " + ", ".join(f"{p} {v:.3f}" for p, v in pc.items()))
 
-    # end to end through the public API: host state in, step, host state out
-    import ctypes  # noqa: F401
-    fields = ("pos", "vel", "u", "h", "rho")
-    host = {f: torch.from_numpy(c.download(f)).pin_memory().numpy() for f in fields}
-    h2d = sum(a.nbytes for a in host.values())
+    # ---- end to end through the public API, chosen form ---------------------
+    fields = {"pos64": np.float64, "vel": np.float32, "u": np.float32, "h": np.float32, "rho": np.float32}
+    host = {}
+    for f, dtp in fields.items():
+        a = cc.download(f)
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        host[f] = (t, t.numpy())
+    h2d = sum(a.nbytes for _, a in host.values())
     d2h = h2d
+    cc.step_all(1, stream)  # graph of one step, captured outside the timed region
+    stream.synchronize()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        for f in fields:
-            c.upload(f, host[f])
-        c.step_all(1)
-        for f in fields:
-            host[f][...] = c.download(f)
-    c.synchronize()
+        for f, (_, a) in host.items():
+            cc.upload_async(f, a, stream)
+        cc.step_all(1, stream)
+        for f, (_, a) in host.items():
+            cc.download_async(f, a, stream)
+        stream.synchronize()
     e2e_s = time.perf_counter() - t0
+    cc.synchronize()
     log(f"e2e: {e2e_s / args.e2e_steps * 1e3:.2f} ms/step")
     e2e_times = torch.tensor([e2e_s], device="cuda")
     if dist is not None:
         dist.all_reduce(e2e_times, op=dist.ReduceOp.MAX)
     e2e_value = world * n * args.e2e_steps / float(e2e_times.item())
 
+    extra = {}
     if rank == 0:
-        dom = max(per_pass, key=per_pass.get)
+        rng = np.random.default_rng(12)
+        targets = rng.choice(n, 16384, replace=False).astype(np.int32)
+        extra["gravity_error"] = {"chosen": gravity_error(cc, targets), "plain": gravity_error(cp, targets)}
+        log(f"gravity error: {extra['gravity_error']}")
+        if args.drift_steps > 0:
+            extra["energy_drift"] = {"plain": energy_drift(cp, args.drift_steps),
+                                     "chosen": energy_drift(cc, args.drift_steps)}
+            dp = extra["energy_drift"]["plain"]["max_rel_change_total_energy"]
+            dc = extra["energy_drift"]["chosen"]["max_rel_change_total_energy"]
+            extra["energy_drift"]["chosen_over_plain"] = dc / dp if dp > 0 else None
+            log(f"energy drift over {args.drift_steps} steps: plain {dp:.3e}, chosen {dc:.3e}")
+
+    if rank == 0:
         peaks = load_peaks()
-        achieved = ALGO_BYTES[dom] * n / (per_pass[dom] / 1e3) / 1e9
+        traffic = load_traffic()
+        dom = max(pc, key=pc.get)
+        achieved = ALGO_BYTES[dom] * n / (pc[dom] / 1e3) / 1e9
+        sweeps = st["sweeps"] / max(st["particles"], 1)
+        # density flops per particle: 20 per neighbour per sweep + 45 per neighbour in the gradient sweep
+        dens_flops = (20.0 * sweeps + 45.0) * 63.0
         line = {
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": K,
-            "warmup": args.warmup, "ms_per_step": elapsed_ms / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded two-body impact generator)",
-            "config": {"workload": f"two-body impact N={n} (800k+200k), leaf {LEAF}, depth {DEPTH}, plain form",
-                       "form": "plain", "n_particles": n, "leaf_capacity": LEAF, "max_tree_depth": DEPTH,
+            "warmup": args.warmup, "ms_per_step": chosen_ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 positions, time and reductions in the chosen form)",
+            "data": "synthetic (seeded two-body impact generator)",
+            "config": {"workload": f"two-body impact N={n} (800k+200k), leaf {LEAF}, depth {DEPTH}",
+                       "form": f"chosen: theta {args.theta} gravity + mixed precision + learned h seed",
+                       "n_particles": n, "leaf_capacity": LEAF, "max_tree_depth": DEPTH,
                        "parallelism": f"replicas x{world}", "l2": "state larger than L2 (no flush)",
-                       "timing": mode},
-            "pass_ms": {p: round(v, 4) for p, v in per_pass.items()},
-            "roofline": {"bound": "hbm", "kernel": f"{dom} pass ({PASS_KERNELS[dom]})", "achieved": achieved,
-                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                         "peak_source": peaks["source"], "algo_bytes_per_particle": ALGO_BYTES[dom],
-                         "traffic": None},
+                       "timing": mode_c},
+            "chosen_over_plain": plain_ms / chosen_ms,
+            "plain": {"value": plain_value, "ms_per_step": plain_ms / K, "timing": mode},
+            "pass_ms": {"chosen": {p: round(v, 4) for p, v in pc.items()},
+                        "plain": {p: round(v, 4) for p, v in pp.items()}},
+            "h_seed": {"sweeps_per_particle": sweeps, "max_sweeps": st["max_sweeps"],
+                       "fallback_rate": st["fallbacks"] / max(st["particles"], 1),
+                       "training_ms_per_call": float(np.mean(train_ms)), "adam_steps_per_call": args.train_iters},
+            "roofline": {"bound": "hbm", "kernel": f"{dom} pass ({PASS_KERNELS[dom]}), chosen form",
+                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                         "algo_bytes_per_particle": ALGO_BYTES[dom],
+                         "traffic": traffic.get(dom, {}).get("bytes_per_launch"),
+                         "traffic_source": traffic.get(dom, {}).get("source"),
+                         "fp32": {"peak_tflops_measured": peak32,
+                                  "density_achieved_tflops": dens_flops * n / (pc["density"] / 1e3) / 1e12,
+                                  "density_flops_per_particle": dens_flops}},
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": launches_per_step(DEPTH) * K,
+                    "d2h_bytes_per_step": int(d2h), "form": "chosen",
+                    "path": "sph_upload_async x5 (pinned), sph_step_all(1), sph_download_async x5, one sync"},
+            "gpu_launches": launches_per_step(DEPTH, True) * K,
             "clocks": clocks,
         }
+        line.update(extra)
         if not args.no_cpu_baseline and world == 1:
             log("cpu baseline ...")
-            cb = cpu_reference(ic, steps=1, warmup=1, budget_s=30.0)
-            log(f"cpu baseline: {cb['value']:.3e} particle-steps/s on {cb['cores']} cores")
-            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            cb = cpu_reference(ic, steps=10, warmup=1, budget_s=20.0)
+            log(f"cpu baseline: {cb['value']:.3e} particle-steps/s on {cb['cores']} threads")
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "physical_cores")}
         print(json.dumps(line), flush=True)
-    c.close()
+    cp.close()
+    cc.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -104,7 +104,9 @@ typedef enum {
     SPH_FIELD_CELL_START = 21,  /* U   _cellStart (2^24), UINT_MAX when empty; download only */
     SPH_FIELD_CELL_END = 22,    /* U   _cellEnd (2^24), 0 when empty; download only */
     SPH_FIELD_POTENTIAL = 23,   /* F   gravitational potential G phi (SPH_GRAVITY_THETA only; no reference buffer) */
-    SPH_FIELD_COUNT = 24
+    SPH_FIELD_POS64 = 24,       /* D3  FP64 master positions (3n doubles) of SPH_PRECISION_MIXED; an upload also
+                                       sets the float positions to their roundings */
+    SPH_FIELD_COUNT = 25
 } sph_field;
 
 /* Defaults equal to SPH/Parameters.h (table paths are the reference's names). */
@@ -304,6 +306,13 @@ sph_status sph_get_buffer(sph_ctx *ctx, sph_field field, void **device_ptr, size
 sph_status sph_synchronize(sph_ctx *ctx, void *stream);
 sph_status sph_get_health(sph_ctx *ctx, uint32_t *word);
 sph_status sph_clear_health(sph_ctx *ctx);
+
+/* Measurement probe (no counterpart in the reference): `blocks` x 256 threads
+ * each run 8 independent FP32 FMA chains of `iters` steps, 16 x iters flops
+ * per thread; sink is device memory of `blocks` floats (written only to keep
+ * the result alive).  Asynchronous on `stream`; time it with events to get the
+ * FP32 FMA peak of the device. */
+sph_status sph_probe_fp32_fma(int32_t blocks, int32_t iters, float *sink, void *stream);
 
 /* Host-only helpers (no GPU work). */
 /* ANEOS.cpp:21-175: parse a table and resample it to res x res (pressure,

@@ -38,7 +38,7 @@ FIELDS = {
     "pos": 0, "vel": 1, "acc": 2, "rho": 3, "u": 4, "mass": 5, "pressure": 6, "h": 7,
     "grad_term": 8, "sound_speed": 9, "du": 10, "balsara": 11, "dhdt": 12, "grav_norm": 13,
     "material": 14, "active": 15, "next_active_time": 16, "global_time": 17, "dt": 18,
-    "cell_key": 19, "cell_index": 20, "cell_start": 21, "cell_end": 22, "potential": 23,
+    "cell_key": 19, "cell_index": 20, "cell_start": 21, "cell_end": 22, "potential": 23, "pos64": 24,
 }
 VECTOR_FIELDS = ("pos", "vel", "acc")
 
@@ -191,6 +191,7 @@ def load(parity: bool = False) -> C.CDLL:
         "sph_hseed_dataset": (st, [vp, _fp, _fp, _fp]),
         "sph_hseed_get_stats": (st, [vp, C.POINTER(SphHSeedStats)]),
         "sph_draw_snapshot": (st, [vp, vp, _ip]),
+        "sph_probe_fp32_fma": (st, [C.c_int32, C.c_int32, vp, vp]),
         "sph_upload": (st, [vp, C.c_int, vp, C.c_size_t]),
         "sph_download": (st, [vp, C.c_int, vp, C.c_size_t]),
         "sph_get_buffer": (st, [vp, C.c_int, C.POINTER(vp), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),

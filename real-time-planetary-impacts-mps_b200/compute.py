@@ -276,6 +276,8 @@ class Compute:
         n = self.nParticles
         if field in _lib.VECTOR_FIELDS:
             out = np.zeros((n, 3), np.float32)
+        elif field == "pos64":
+            out = np.zeros((n, 3), np.float64)
         elif field in ("global_time", "dt"):
             out = np.zeros(1, np.int32)
         elif field in ("material", "next_active_time"):
@@ -295,6 +297,8 @@ class Compute:
     def upload(self, field: str, values) -> None:
         if field in _lib.VECTOR_FIELDS:
             a = np.ascontiguousarray(np.asarray(values, np.float32).reshape(-1))
+        elif field == "pos64":
+            a = np.ascontiguousarray(np.asarray(values, np.float64).reshape(-1))
         elif field in ("global_time", "dt", "material", "next_active_time"):
             a = np.ascontiguousarray(np.asarray(values, np.int32).reshape(-1))
         elif field == "active":

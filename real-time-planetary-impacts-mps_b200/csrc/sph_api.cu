@@ -53,6 +53,38 @@ __global__ void k_get_w(const float4 *__restrict__ src, float *__restrict__ dst,
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = src[i].w;
 }
+__global__ void k_pack3d(const double *__restrict__ src, double4 *__restrict__ dst64, float4 *__restrict__ dst,
+                         int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = src[3 * i], y = src[3 * i + 1], z = src[3 * i + 2];
+    dst64[i] = make_double4(x, y, z, 0.0);
+    const float w = dst[i].w;
+    dst[i] = make_float4((float)x, (float)y, (float)z, w);
+}
+__global__ void k_unpack3d(const double4 *__restrict__ src, double *__restrict__ dst, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 v = src[i];
+    dst[3 * i] = v.x;
+    dst[3 * i + 1] = v.y;
+    dst[3 * i + 2] = v.z;
+}
+// FP32 FMA throughput probe: 8 independent FMA chains per thread.
+__global__ void __launch_bounds__(256) k_fma_probe(int iters, float seed, float *sink) {
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = seed + (float)(threadIdx.x + k);
+    const float m = 0.999999f, c = 1e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], m, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == 1234.5678f) sink[blockIdx.x] = s;  // keeps the chains alive
+}
 __global__ void k_time_to64(const int32_t *globals, double *dglob) {
     dglob[0] = (double)kDtMin1 * (double)globals[0];
 }
@@ -345,7 +377,7 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     chk(dmalloc(&ctx->cell_range, (size_t)kNumCells));
     for (float4 **fp : {&ctx->sp4, &ctx->sv4, &ctx->sA, &ctx->sB, &ctx->sC}) chk(dmalloc(fp, n));    chk(dmalloc(&ctx->eos_forsterite, (size_t)res * res));
     chk(dmalloc(&ctx->eos_fe, (size_t)res * res));
-    ctx->stage_bytes = std::max((size_t)kNumCells * sizeof(uint32_t), sizeof(float) * 3 * (size_t)n);
+    ctx->stage_bytes = std::max((size_t)kNumCells * sizeof(uint32_t), sizeof(double) * 3 * (size_t)n);
     chk(cudaMalloc(&ctx->stage, ctx->stage_bytes));
     chk(dmalloc(&ctx->snapshot, (size_t)kSnapshotRes * kSnapshotRes));
     chk(dmalloc(&ctx->dglob, 4));
@@ -449,6 +481,26 @@ sph_status sph_upload_async(sph_ctx *ctx, sph_field field, const void *host, siz
                 return launch_pos_to64(ctx, st);
             return cuda_status(e, "sph_upload");
         }
+        case SPH_FIELD_POS64: {
+            if (ctx->form.precision != SPH_PRECISION_MIXED || !ctx->pos64) {
+                set_error("sph_upload: FP64 positions exist in the mixed-precision form only");
+                return SPH_ERR_INVALID_ARG;
+            }
+            if (count != need3) {
+                set_error("sph_upload: FP64 positions expect %zu doubles, got %zu", need3, count);
+                return SPH_ERR_INVALID_ARG;
+            }
+            if (sizeof(double) * count > ctx->stage_bytes) {
+                set_error("sph_upload: FP64 positions exceed the staging buffer");
+                return SPH_ERR_INVALID_ARG;
+            }
+            cudaError_t e = cudaMemcpyAsync(ctx->stage, host, sizeof(double) * count, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) {
+                k_pack3d<<<blocks, 256, 0, st>>>((const double *)ctx->stage, ctx->pos64, ctx->pos4, n);
+                e = cudaGetLastError();
+            }
+            return cuda_status(e, "sph_upload");
+        }
         case SPH_FIELD_MASS: {
             if (count != need1) {
                 set_error("sph_upload: mass expects %zu floats", need1);
@@ -538,6 +590,18 @@ sph_status sph_download_async(sph_ctx *ctx, sph_field field, void *host, size_t 
             return cuda_status(cudaMemcpyAsync(host, ctx->stage, sizeof(float) * count, cudaMemcpyDeviceToHost, st),
                                "sph_download");
         }
+        case SPH_FIELD_POS64:
+            if (ctx->form.precision != SPH_PRECISION_MIXED || !ctx->pos64) {
+                set_error("sph_download: FP64 positions exist in the mixed-precision form only");
+                return SPH_ERR_INVALID_ARG;
+            }
+            if (count != 3 * (size_t)n || sizeof(double) * count > ctx->stage_bytes) {
+                set_error("sph_download: FP64 positions expect %d doubles", 3 * n);
+                return SPH_ERR_INVALID_ARG;
+            }
+            k_unpack3d<<<blocks, 256, 0, st>>>(ctx->pos64, (double *)ctx->stage, n);
+            return cuda_status(cudaMemcpyAsync(host, ctx->stage, sizeof(double) * count, cudaMemcpyDeviceToHost, st),
+                               "sph_download");
         case SPH_FIELD_MASS:
             if (count != (size_t)n) {
                 set_error("sph_download: mass expects %d floats", n);
@@ -622,6 +686,7 @@ sph_status sph_get_buffer(sph_ctx *ctx, sph_field field, void **device_ptr, size
         case SPH_FIELD_CELL_INDEX: p = ctx->cell_sort.vals[ctx->cell_final]; b = 4 * n; break;
         case SPH_FIELD_CELL_START: p = ctx->cell_range; b = 8 * (size_t)kNumCells; s = 8; break;
         case SPH_FIELD_CELL_END: p = (char *)ctx->cell_range + 4; b = 8 * (size_t)kNumCells; s = 8; break;
+        case SPH_FIELD_POS64: p = ctx->pos64; b = 32 * n; s = 32; break;
         default: return SPH_ERR_INVALID_ARG;
     }
     *device_ptr = p;
@@ -991,6 +1056,12 @@ sph_status sph_step_all(sph_ctx *ctx, void *stream, int32_t n_steps) {
         if (e != cudaSuccess) return cuda_status(e, "graph launch");
     }
     return SPH_OK;
+}
+
+sph_status sph_probe_fp32_fma(int32_t blocks, int32_t iters, float *sink, void *stream) {
+    if (blocks < 1 || iters < 1 || !sink) return SPH_ERR_INVALID_ARG;
+    k_fma_probe<<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, 0.5f, sink);
+    return cuda_status(cudaGetLastError(), "sph_probe_fp32_fma");
 }
 
 sph_status sph_draw_snapshot(sph_ctx *ctx, void *stream, int32_t *image) {
