@@ -32,6 +32,17 @@ namespace {
 // floor(x / CELL_WIDTH); 2e-4 Mm keeps every particle of a cell inside its box.
 constexpr float kCellMargin = 2e-4f;
 
+// Square root of a pair distance.  The parity build keeps the correctly
+// rounded sqrtf of the reference; the product uses the hardware reciprocal
+// square root (within 2 ulp), a rounding-level difference.
+__device__ __forceinline__ float pair_sqrt(float r2) {
+#ifdef SPH_PARITY
+    return sqrtf(r2);
+#else
+    return r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+#endif
+}
+
 // Lanes per particle in the density and acceleration walks.  The parity
 // build (SPH_PARITY) uses one, which sums in the reference's sequential order.
 #ifdef SPH_PARITY
@@ -346,12 +357,13 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArg
         float part = 0.f;
         int found = 0;
         if (n_list <= kListMax) {
+#pragma unroll 4
             for (int i = sub; i < n_list; i += L) {
                 const float4 q = __ldg(sp4 + list[i]);
                 const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
                 const float r2 = dx * dx + dy * dy + dz * dz;
                 if (r2 > hs2x4) continue;
-                const float r = sqrtf(r2);
+                const float r = pair_sqrt(r2);
                 if (cached && r > h2) continue;
                 ++found;
                 part += kernel_w(r, h1) * q.w;
@@ -362,7 +374,7 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArg
                 const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
                 const float r2 = dx * dx + dy * dy + dz * dz;
                 if (r2 > hs2x4) return;
-                const float r = sqrtf(r2);
+                const float r = pair_sqrt(r2);
                 if (cached && r > h2) return;
                 ++found;
                 part += kernel_w(r, h1) * q.w;
@@ -423,13 +435,14 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArg
     };
     if (n_list <= kListMax && g2 > list_r2) build(gh);
     if (n_list <= kListMax) {
+#pragma unroll 4
         for (int i = sub; i < n_list; i += L) {
             const uint32_t k = list[i];
             const float4 q = __ldg(sp4 + k);
             const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
             const float r2 = dx * dx + dy * dy + dz * dz;
             if (r2 > g2) continue;
-            const float r = sqrtf(r2);
+            const float r = pair_sqrt(r2);
             if (gcached && r > h2) continue;
             grad(k, r, q.w, dx, dy, dz);
         }
@@ -439,7 +452,7 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArg
             const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
             const float r2 = dx * dx + dy * dy + dz * dz;
             if (r2 > g2) return;
-            const float r = sqrtf(r2);
+            const float r = pair_sqrt(r2);
             if (gcached && r > h2) return;
             grad(k, r, q.w, dx, dy, dz);
         });
@@ -545,7 +558,7 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_acceleration(Accel
                 const float hj = Aj.w;
                 const float4 Cj = __ldg(sC + k);
                 const float4 Bj = __ldg(sB + k);
-                const float r = sqrtf(r2);
+                const float r = pair_sqrt(r2);
                 const float r1 = 1.f / r;
                 const float mj = Cj.x, factj = Cj.y, rhoj = Cj.z, Balj = Cj.w;
                 const float hj1 = 1.f / hj;

@@ -77,7 +77,7 @@ def test_learned_seed_against_plain_guess(cuda, pkg):
         gt, dt = c.download("global_time"), c.download("dt")
         s = torch.cuda.Stream()
         res = {}
-        for tol in (0.0, 2e-7):
+        for tol in (0.0, 1e-7):
             for seed in ("plain", "learned"):
                 def restore():
                     for f, v in state.items():
@@ -107,7 +107,7 @@ def test_learned_seed_against_plain_guess(cuda, pkg):
         assert res[(0.0, "learned")]["sweeps"] < res[(0.0, "plain")]["sweeps"]
         assert res[(0.0, "learned")]["fallback"] < 0.05
         # iterated tightly, both starts converge to the same h
-        a, b = res[(2e-7, "learned")]["h"].astype(np.float64), res[(2e-7, "plain")]["h"].astype(np.float64)
+        a, b = res[(1e-7, "learned")]["h"].astype(np.float64), res[(1e-7, "plain")]["h"].astype(np.float64)
         rel = np.abs(a - b) / b
         print(f"  tight tolerance: converged h max relative difference {rel.max():.2e}")
         assert rel.max() <= 1e-6
