@@ -253,17 +253,20 @@ def graph_time(c, stream, K: int) -> tuple[float, str]:
     return t0.elapsed_time(t1), mode
 
 
-def pass_times(c, stream, K: int) -> dict:
-    """Per-pass device times (ms), eager with events between the passes."""
+def pass_times(c, stream, K: int, label: str) -> dict:
+    """Per-pass device times (ms), eager with events between the passes; the
+    launches sit in an NVTX range named `label` (for profiler filters)."""
     import torch
     calls = (c.updateOctreeBuffer, c.sort, c.gravitationalPass, c.densityPass, c.accelerationPass, c.stepPass)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(PASSES) + 1)] for _ in range(K)]
+    torch.cuda.nvtx.range_push(label)
     with torch.cuda.stream(stream):
         for k in range(K):
             ev[k][0].record(stream)
             for j, f in enumerate(calls):
                 f(stream)
                 ev[k][j + 1].record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     c.synchronize()
     return {p: sum(ev[k][j].elapsed_time(ev[k][j + 1]) for k in range(K)) / K for j, p in enumerate(PASSES)}
@@ -409,8 +412,8 @@ def main():
     plain_value = world * n * K / (plain_ms / 1e3)
     log(f"timed: plain {plain_ms / K:.3f} ms/step, chosen {chosen_ms / K:.3f} ms/step")
 
-    pp = pass_times(cp, stream, K)
-    pc = pass_times(cc, stream, K)
+    pp = pass_times(cp, stream, K, "plain_passes")
+    pc = pass_times(cc, stream, K, "chosen_passes")
     st = cc.hseed_stats()
     log("plain  per-pass ms: " + ", ".join(f"{p} {v:.3f}" for p, v in pp.items()))
     log("chosen per-pass ms: " + ", ".join(f"{p} {v:.3f}" for p, v in pc.items()))

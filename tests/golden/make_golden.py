@@ -13,6 +13,7 @@ fixtures are committed so the tests run without it.
 """
 from __future__ import annotations
 
+import hashlib
 import importlib
 import os
 import sys
@@ -36,6 +37,9 @@ PASS_OUTPUTS = {
     "acceleration": ("acc", "du", "dhdt", "next_active_time", "dt"),
     "step": ("pos", "vel", "u", "h", "rho", "global_time"),
 }
+
+
+C0_STEPS = 10
 
 
 def occupied_cells(st) -> np.ndarray:
@@ -84,6 +88,22 @@ def main(ref_root: str | None = None):
             for f in fields:
                 out[f"s{s}_{p}_{f}"] = getattr(st, f).copy()
     np.savez_compressed(os.path.join(HERE, "steps_impact_2560.npz"), **out)
+    # 5. config 0 as stated (16384 + 4096, leaf capacity 32): ten full steps,
+    # every pass, the reference's CPU octree rebuilt from the current
+    # positions each step; SHA-256 of every output array per pass per step
+    ic = pkg_ic.make_impact(16384, 4096, seed=0)
+    st = O.OracleState(ic, ef, ee, kind="ref")
+    digests, names = [], []
+    for s in range(C0_STEPS):
+        st.set_tree(O.tree_reference(st.pos, 32, kind="ref"))
+        for p, fields in PASS_OUTPUTS.items():
+            getattr(st, p)()
+            for f in fields:
+                digests.append(np.frombuffer(hashlib.sha256(np.ascontiguousarray(getattr(st, f)).tobytes()).digest(),
+                                             np.uint8))
+                names.append(f"s{s}_{p}_{f}")
+    np.savez_compressed(os.path.join(HERE, "config0_digests.npz"), names=np.array(names), digests=np.stack(digests),
+                        final_pos=st.pos, final_vel=st.vel, final_u=st.u, final_h=st.h, final_rho=st.rho)
     print("fixtures written to", HERE)
 
 

@@ -41,6 +41,13 @@ P99_TOL = {"acc": 1e-3, "grav_norm": 1e-3, "vel": 1e-4}
 # differ from the reference's sequential ones by rounding: ~5e-7 relative on
 # density, which the steep EOS table turns into up to ~1e-4 on pressure.
 TOL_PRODUCT = dict(TOL, pressure=5e-4, sound_speed=5e-4, balsara=1e-3, du=1e-3, dhdt=1e-3)
+# The parity build (-fmad=false, sequential sums) rounds like the reference:
+# 1e-5 everywhere except the EOS outputs, where one ulp of logf/powf (CUDA
+# against glibc) in the table coordinate moves pressure by up to ~6e-5 on the
+# steep parts of the table, and du/dt, which carries pressure.
+TOL_PARITY = {"acc": 1e-5, "grav_norm": 1e-5, "h": 1e-5, "rho": 1e-5, "grad_term": 1e-5, "pressure": 1e-4,
+              "sound_speed": 1e-5, "balsara": 1e-5, "du": 1e-4, "dhdt": 1e-5, "pos": 1e-6, "vel": 1e-5, "u": 1e-5}
+P99_TOL_PARITY = {}
 PASS_METHOD = {"sort": "sort", "gravity": "gravitationalPass", "density": "densityPass",
                "acceleration": "accelerationPass", "step": "stepPass"}
 
@@ -59,8 +66,9 @@ def rel_err(a, b):
     return d / np.maximum(m, floor)
 
 
-def compare(field, got, want, where, tol=None):
+def compare(field, got, want, where, tol=None, p99=None):
     tol = TOL if tol is None else tol
+    p99 = P99_TOL if p99 is None else p99
     if field in INT_FIELDS:
         bad = np.nonzero(np.asarray(got).reshape(-1) != np.asarray(want).reshape(-1))[0]
         assert bad.size == 0, f"{where} {field}: {bad.size} mismatches, first at {bad[:5]}"
@@ -70,9 +78,9 @@ def compare(field, got, want, where, tol=None):
     print(f"  {where:28s} {field:12s} max rel err {worst:.3e}  p99 {np.percentile(e, 99):.3e}")
     assert np.all(np.isfinite(np.asarray(got))), f"{where} {field}: non-finite values"
     assert worst <= tol[field], f"{where} {field}: max rel err {worst:.3e} > {tol[field]:.1e}"
-    if field in P99_TOL and e.size:
-        p99 = float(np.percentile(e, 99))
-        assert p99 <= P99_TOL[field], f"{where} {field}: p99 rel err {p99:.3e} > {P99_TOL[field]:.1e}"
+    if field in p99 and e.size:
+        q = float(np.percentile(e, 99))
+        assert q <= p99[field], f"{where} {field}: p99 rel err {q:.3e} > {p99[field]:.1e}"
     return worst
 
 
@@ -122,7 +130,8 @@ def test_every_pass_matches_reference_two_steps(cuda, pkg, build):
     parity = build == "parity"
     if parity:
         pkg.build(parity=True)
-    tol = TOL if parity else TOL_PRODUCT
+    tol = TOL_PARITY if parity else TOL_PRODUCT
+    p99 = P99_TOL_PARITY if parity else P99_TOL
     with pkg.Compute(ic, tree_source="host", max_children_in_leaf=8, parity=parity) as c:
         for s in range(2):
             if s == 1:
@@ -140,7 +149,7 @@ def test_every_pass_matches_reference_two_steps(cuda, pkg, build):
                 getattr(c, PASS_METHOD[p])()
                 c.synchronize()
                 for f in fields:
-                    compare(f, c.download(f), g[f"s{s}_{p}_{f}"], f"{build} step {s} {p}", tol)
+                    compare(f, c.download(f), g[f"s{s}_{p}_{f}"], f"{build} step {s} {p}", tol, p99)
 
 
 def test_gpu_tree_matches_oracle_morton_tree(cuda, pkg, O):
@@ -219,3 +228,99 @@ def test_snapshot_splat(cuda, pkg):
     want = np.zeros(1024 * 1024, np.int64)
     np.maximum.at(want, px, ic["material"][ok].astype(np.int64))
     assert np.array_equal(img.reshape(-1), want.astype(np.int32))
+
+
+STATE = ("pos", "vel", "u", "h", "rho", "pressure", "grad_term", "sound_speed", "balsara", "grav_norm", "active",
+         "next_active_time", "global_time")
+
+
+def upload_state(c, st):
+    for f in STATE:
+        c.upload(f, getattr(st, f))
+
+
+@pytest.mark.parametrize("build", ["parity", "product"])
+def test_config0_ten_steps_every_pass(cuda, pkg, O, eos_grids, build):
+    """Config 0 as stated (16384 + 4096 particles, leaf capacity 32), ten
+    steps: every pass of the CUDA path against the oracle (pinned bit-exact to
+    the reference's own kernels over these ten steps by
+    test_oracle_golden.py), on the reference's octree; each step restarts
+    the GPU from the oracle's state so that differences do not compound."""
+    parity = build == "parity"
+    if parity:
+        pkg.build(parity=True)
+    tol = TOL_PARITY if parity else TOL_PRODUCT
+    p99 = P99_TOL_PARITY if parity else P99_TOL
+    ic = pkg.ic.make_impact(16384, 4096, seed=0)
+    st = O.OracleState(ic, *eos_grids)
+    worst = {}
+    print()
+    with pkg.Compute(ic, tree_source="host", max_children_in_leaf=32, parity=parity) as c:
+        for s in range(10):
+            t = O.tree_reference(st.pos, 32)
+            st.set_tree(t)
+            upload_state(c, st)
+            c.set_tree(t)
+            for p, fields in PASS_OUTPUTS.items():
+                getattr(st, p)()
+                getattr(c, PASS_METHOD[p])()
+                c.synchronize()
+                for f in fields:
+                    e = compare(f, c.download(f), getattr(st, f), f"{build} c0 step {s} {p}", tol, p99)
+                    worst[f] = max(worst.get(f, 0.0), e)
+    print("  worst over ten steps:", {k: f"{v:.1e}" for k, v in worst.items()})
+
+
+def test_sort_cells_and_tree_structure_at_1e6(cuda, pkg):
+    """Size-independent checks at N = 10^6 (the benchmark impact): the sort
+    is a stable permutation with non-decreasing keys that equal the hash of
+    each particle's position; the cell table covers [0, N) exactly, one range
+    per occupied key; the GPU tree's leaves hold every particle exactly once."""
+    ic = pkg.ic.make_impact(800000, 200000, seed=0)
+    n = int(ic["n"])
+    with pkg.Compute(ic, max_children_in_leaf=32, max_tree_depth=7) as c:
+        c.step()
+        c.updateOctreeBuffer()
+        c.sort()
+        c.synchronize()
+        pos = c.download("pos")
+        key, idx = c.download("cell_key"), c.download("cell_index")
+        # permutation, sorted keys, stability
+        assert np.array_equal(np.sort(idx), np.arange(n, dtype=np.uint32))
+        assert np.all(np.diff(key.astype(np.int64)) >= 0)
+        same = np.diff(key.astype(np.int64)) == 0
+        assert np.all(np.diff(idx.astype(np.int64))[same] > 0)
+        # keys are the hash of the positions (sort.metal:15-44)
+        cell = np.floor(pos / np.float32(0.18)).astype(np.int64) & 255
+
+        def spread(v):
+            v = v & 0x3FF
+            v = (v | (v << 16)) & 0x030000FF
+            v = (v | (v << 8)) & 0x0300F00F
+            v = (v | (v << 4)) & 0x030C30C3
+            return (v | (v << 2)) & 0x09249249
+
+        want = spread(cell[:, 0]) | (spread(cell[:, 1]) << 1) | (spread(cell[:, 2]) << 2)
+        assert np.array_equal(key.astype(np.int64), want[idx])
+        # cell ranges: one (first, last) per run of equal keys, empty elsewhere
+        start, end = c.download("cell_start"), c.download("cell_end")
+        first = np.concatenate([[True], np.diff(key.astype(np.int64)) != 0])
+        last = np.concatenate([np.diff(key.astype(np.int64)) != 0, [True]])
+        occ = key[first]
+        assert np.array_equal(start[occ], np.nonzero(first)[0].astype(np.uint32))
+        assert np.array_equal(end[occ], np.nonzero(last)[0].astype(np.uint32))
+        assert int((end[occ].astype(np.int64) - start[occ] + 1).sum()) == n
+        empty = np.ones(1 << 24, bool)
+        empty[occ] = False
+        assert np.all(start[empty] == 0xFFFFFFFF) and np.all(end[empty] == 0)
+        # tree: leaf membership is a permutation
+        t = c.get_tree()
+        T = t["tree"]
+        members = []
+        for off in t["level_nodes"]:
+            cnt = T[off]
+            if cnt > 0:
+                members.append(T[off + 2:off + 2 + cnt])
+        members = np.concatenate(members)
+        assert members.size == n
+        assert np.array_equal(np.sort(members), np.arange(n, dtype=np.int32))
