@@ -377,7 +377,9 @@ def main():
             cc.step(stream)
             stream.synchronize()
             t0 = time.perf_counter()
+            torch.cuda.nvtx.range_push("seed_training")
             cc.hseed_train(args.train_iters, 16384, 1e-3, stream)
+            torch.cuda.nvtx.range_pop()
             train_ms.append((time.perf_counter() - t0) * 1e3)
     cc.hseed_capture(False)
     cc.set_form(gravity="theta", theta=args.theta, precision="mixed", h_seed="learned")
