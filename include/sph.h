@@ -211,6 +211,8 @@ typedef struct {
     uint32_t fallbacks;  /* particles whose learned seed was abandoned */
     uint32_t max_sweeps; /* most sweeps of one particle */
     uint32_t particles;  /* particles iterated */
+    uint32_t tiles;      /* occupied cell octets the product build's density pass staged */
+    uint32_t deferred;   /* particles it handed from the tiles to the per-particle walk */
 } sph_hseed_stats;
 int32_t sph_hseed_num_params(void);
 sph_status sph_hseed_capture(sph_ctx *ctx, int32_t on);

@@ -77,7 +77,7 @@ class SphForm(C.Structure):
 
 class SphHSeedStats(C.Structure):
     _fields_ = [("sweeps", C.c_uint32), ("fallbacks", C.c_uint32), ("max_sweeps", C.c_uint32),
-                ("particles", C.c_uint32)]
+                ("particles", C.c_uint32), ("tiles", C.c_uint32), ("deferred", C.c_uint32)]
 
 
 SPH_HSEED_PLAIN = 0

@@ -243,7 +243,8 @@ class Compute:
         """Counters of the last density pass's h iteration."""
         st = _lib.SphHSeedStats()
         self._check(self._lib.sph_hseed_get_stats(self._h, C.byref(st)), "sph_hseed_get_stats")
-        return dict(sweeps=st.sweeps, fallbacks=st.fallbacks, max_sweeps=st.max_sweeps, particles=st.particles)
+        return dict(sweeps=st.sweeps, fallbacks=st.fallbacks, max_sweeps=st.max_sweeps, particles=st.particles,
+                    tiles=st.tiles, deferred=st.deferred)
 
     def diagnostics(self, stream=None, theta_potential: float = 0.5) -> dict:
         """FP64 conservation sums (mass, energies, momentum, angular momentum)."""

@@ -306,7 +306,7 @@ sph_status sph_destroy(sph_ctx *ctx) {
                     ctx->du, ctx->B, ctx->dhdt, ctx->gnorm, ctx->phi, ctx->mat, ctx->nat, ctx->active, ctx->globals,
                     ctx->health, ctx->cell_range, ctx->sp4, ctx->sv4, ctx->sA, ctx->sB, ctx->sC,
                     ctx->eos_forsterite, ctx->eos_fe, ctx->stage, ctx->snapshot, ctx->pos64, ctx->dglob,
-                    ctx->diag};
+                    ctx->diag, ctx->tiles, ctx->tile_ctr, ctx->deferred};
     for (void *b : bufs) cudaFree(b);
     sort_free(ctx->cell_sort);
     hseed_free(ctx);
@@ -382,6 +382,9 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     chk(dmalloc(&ctx->snapshot, (size_t)kSnapshotRes * kSnapshotRes));
     chk(dmalloc(&ctx->dglob, 4));
     chk(dmalloc(&ctx->diag, (size_t)kDiagDoubles));
+    chk(dmalloc(&ctx->tiles, (size_t)n));
+    chk(dmalloc(&ctx->tile_ctr, 4));
+    chk(dmalloc(&ctx->deferred, (size_t)n));
     if (e != cudaSuccess) {
         s = cuda_status(e, "sph_create allocation");
         sph_destroy(ctx);

@@ -43,6 +43,17 @@ __device__ __forceinline__ float pair_sqrt(float r2) {
 #endif
 }
 
+// 1 / r for a pair at r = pair_sqrt(r2) > 0: the correctly rounded quotient
+// in the parity build, the hardware reciprocal square root in the product.
+__device__ __forceinline__ float pair_rinv(float r2, float r) {
+#ifdef SPH_PARITY
+    return 1.f / r;
+#else
+    (void)r;
+    return rsqrtf(r2);
+#endif
+}
+
 // Lanes per particle in the density and acceleration walks.  The parity
 // build (SPH_PARITY) uses one, which sums in the reference's sequential order.
 #ifdef SPH_PARITY
@@ -274,18 +285,11 @@ constexpr float kListReach = 1.15f; // list radius / (2 h)
 // density.metal:12-239 for one sorted particle per lane group.  The group
 // keeps the reference's per-particle iteration state (h, the int max_h, the
 // cached scan's h and neighbour count) identically in all its lanes.
+// w_off / w_start: the warp's 32-entry walk scratch; list: the group's
+// kListMax-entry neighbour list.
 template <int L>
-__global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArgs a) {
-    extern __shared__ uint32_t s_lists[];
-    __shared__ uint32_t s_off[parts_per_block<L>() * L], s_start[parts_per_block<L>() * L];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31, sub = lane & (L - 1), gbase = lane & ~(L - 1);
-    uint32_t *w_off = s_off + (threadIdx.x & ~31), *w_start = s_start + (threadIdx.x & ~31);
-    uint32_t *list = s_lists + (size_t)(threadIdx.x / L) * kListMax;
-    const unsigned gm = group_mask<L>(lane);
-    const int index = t / L;
-    if (index >= a.n) return;  // whole groups leave together
-    if (t == 0) a.globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
+__device__ __forceinline__ void density_particle(const DensityArgs &a, int index, int sub, unsigned gm, int gbase,
+                                                 uint32_t *w_off, uint32_t *w_start, uint32_t *list) {
     const uint32_t ind = a.cidx[index];
     const float4 me = a.sp4[index];
     const float4 mv = a.sv4[index];
@@ -495,6 +499,615 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArg
     a.sA[index] = make_float4(px, py, pz, hi);
     a.sB[index] = make_float4(vix, viy, viz, pc.y);
     a.sC[index] = make_float4(mi, (fi * pc.x / (dens * dens)), dens, bal);
+}
+
+// One lane group per sorted particle, every particle.
+template <int L>
+__global__ void __launch_bounds__(parts_per_block<L>() * L) k_density(DensityArgs a) {
+    extern __shared__ uint32_t s_lists[];
+    __shared__ uint32_t s_off[parts_per_block<L>() * L], s_start[parts_per_block<L>() * L];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, sub = lane & (L - 1), gbase = lane & ~(L - 1);
+    const int index = t / L;
+    if (index >= a.n) return;  // whole groups leave together
+    if (t == 0) a.globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
+    density_particle<L>(a, index, sub, group_mask<L>(lane), gbase, s_off + (threadIdx.x & ~31),
+                        s_start + (threadIdx.x & ~31), s_lists + (size_t)(threadIdx.x / L) * kListMax);
+}
+
+// The particles the tile pass handed on (sorted indices idx[0, *count)),
+// one lane group each, grid-stride.
+template <int L>
+__global__ void __launch_bounds__(parts_per_block<L>() * L)
+    k_density_deferred(DensityArgs a, const uint32_t *__restrict__ idx, const uint32_t *__restrict__ count) {
+    extern __shared__ uint32_t s_lists[];
+    __shared__ uint32_t s_off[parts_per_block<L>() * L], s_start[parts_per_block<L>() * L];
+    const int lane = threadIdx.x & 31, sub = lane & (L - 1), gbase = lane & ~(L - 1);
+    const uint32_t cnt = *count;
+    constexpr int per_block = parts_per_block<L>();
+    for (uint32_t base = blockIdx.x * per_block; base < cnt; base += gridDim.x * per_block) {
+        const uint32_t j = base + threadIdx.x / L;
+        if (j < cnt)
+            density_particle<L>(a, (int)idx[j], sub, group_mask<L>(lane), gbase, s_off + (threadIdx.x & ~31),
+                                s_start + (threadIdx.x & ~31), s_lists + (size_t)(threadIdx.x / L) * kListMax);
+    }
+}
+
+// ---- density over cell tiles (product build) --------------------------------
+//
+// A tile is an aligned Morton block of cells -- 64 cells (4 x 4 x 4), or, where
+// such a block holds many particles, its 16-cell halves of halves or its
+// octets -- so its particles are one contiguous run of the sorted order.  A CTA
+// takes tiles from a ticket counter; per tile it stages, once, every particle
+// of the box of cells that the tile's neighbour lists can reach (float4
+// position + mass and the sorted index) into shared memory, in cell order
+// x-major, then y, z innermost, so a row of cells along z is one contiguous
+// run of staged slots.  Warps then take the tile's particles four at a time
+// (density_tile_warp): the list build reads the particles' rows of the staged
+// box, every h-iteration sweep reads the list, and no sweep touches the cell
+// table or global positions again.  A particle whose list box reaches more
+// than kTileReach cells beyond its own cell, whose h is at least
+// MAX_SMOOTHING_LENGTH (where the reference's neighbour cache comes into play),
+// whose list overflows or whose growing h leaves the staged box is handed to
+// k_density_deferred, which runs the per-particle walk above; so is every
+// particle of a tile whose box exceeds the shared-memory budget.
+constexpr int kTileThreads = 384;
+constexpr int kTileLanes = 8;                               // lanes per particle
+constexpr int kTileGroups = kTileThreads / kTileLanes;      // particles in flight per CTA
+constexpr int kTileStageMax = 3840;                         // staged particles per tile
+constexpr int kTileCellsMax = 1024;                         // cells of a tile's staged box
+constexpr int kTileCellsPerThread = (kTileCellsMax + kTileThreads - 1) / kTileThreads;
+constexpr int kTileReach = 3;                               // cells a list box may extend past its own cell
+constexpr int kTileList = 256;                              // list entries per particle (staged slots)
+constexpr uint32_t kTileBlockMax = 320;                     // particles of a 64-cell tile
+constexpr uint32_t kTileHalfMax = 256;                      // particles of a 16-cell tile
+
+struct TileShared {
+    float4 pos[kTileStageMax];          // staged (x, y, z, m)
+    uint32_t gidx[kTileStageMax];       // staged sorted index
+    uint32_t off[kTileCellsMax + 1];    // first staged slot of each box cell; off[cells] = staged count
+    uint32_t first[kTileCellsMax];      // first sorted index of each box cell
+    uint16_t list[kTileGroups][kTileList];
+    int box[6];                         // staged box: lo x y z, hi x y z (unwrapped cell coordinates)
+    uint32_t wsum[kTileThreads / 32];
+    uint32_t start, end, tile, next;
+    uint32_t stats[4];
+    int defer_all;
+};
+
+// The list box of a tile particle at smoothing length hb -- the cells within
+// 2 hb kListReach, widened by 1e-3 of a cell so that float rounding of the
+// cell coordinates (|x| / CELL_WIDTH < 2^12, a few 1e-4 of a cell) never drops
+// a cell -- and whether the tile path can take the particle (reach within
+// kTileReach cells of its own, h < MAX_H).
+__device__ __forceinline__ bool tile_box(float px, float py, float pz, float hb, CellBox &b) {
+    constexpr float iw = 1.f / kCellWidth;
+    constexpr float widen = 1e-3f;
+    const float rl = 2.f * hb * kListReach;
+    b.lo0 = (int)floorf((px - rl) * iw - widen);
+    b.lo1 = (int)floorf((py - rl) * iw - widen);
+    b.lo2 = (int)floorf((pz - rl) * iw - widen);
+    b.hi0 = (int)floorf((px + rl) * iw + widen);
+    b.hi1 = (int)floorf((py + rl) * iw + widen);
+    b.hi2 = (int)floorf((pz + rl) * iw + widen);
+    const int ox = (int)floorf(px * iw), oy = (int)floorf(py * iw), oz = (int)floorf(pz * iw);
+    return hb < kMaxH && ox - b.lo0 <= kTileReach && b.hi0 - ox <= kTileReach && oy - b.lo1 <= kTileReach &&
+           b.hi1 - oy <= kTileReach && oz - b.lo2 <= kTileReach && b.hi2 - oz <= kTileReach;
+}
+
+// The starting h of an active particle's iteration (the learned seed when it
+// is accepted, as in density_particle) and the h its staged box is built for.
+__device__ __forceinline__ float tile_start_h(const DensityArgs &a, uint32_t ind, float h_plain, bool &seeded) {
+    seeded = false;
+    if (a.seed) {
+        const float sd = a.seed[ind];
+        if (sd >= 0.5f * h_plain && sd <= 2.f * h_plain && sd <= kMaxH) {
+            seeded = true;
+            return sd;
+        }
+    }
+    return h_plain;
+}
+
+// Tiles: at the first sorted particle of every occupied 64-cell block, the
+// block's octet ranges (from its 64 cell ranges); the block is one tile when it
+// holds at most kTileBlockMax particles, else each 16-cell quarter is one when
+// it holds at most kTileHalfMax, else each octet is.  (first, one past last)
+// per tile, in ticket order.  ctr[0] counts tiles; ctr[1] is the CTAs' tile
+// ticket, ctr[2] the deferred count.
+__global__ void k_tile_starts(int n, const uint32_t *__restrict__ skey, const uint2 *__restrict__ cells,
+                              uint2 *__restrict__ tiles, uint32_t *ctr, int32_t *globals) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0) globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
+    if (k >= n) return;
+    const uint32_t blk = skey[k] >> 6;
+    if (k > 0 && (skey[k - 1] >> 6) == blk) return;
+    uint32_t ofirst[8], oend[8];  // octet ranges; oend == 0 when empty
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        uint32_t f = 0xffffffffu, l = 0u;
+        for (int j = 0; j < 8; ++j) {
+            const uint2 r = cells[blk * 64u + (uint32_t)(o * 8 + j)];
+            if (r.x != 0xffffffffu) {
+                f = min(f, r.x);
+                l = max(l, r.y + 1u);
+            }
+        }
+        ofirst[o] = f;
+        oend[o] = l;
+    }
+    auto emit = [&](uint32_t f, uint32_t l) {
+        if (l > f) tiles[atomicAdd(ctr, 1u)] = make_uint2(f, l);
+    };
+    auto span = [&](int o0, int o1, uint32_t &f, uint32_t &l) {  // octets o0 .. o1 - 1
+        f = 0xffffffffu;
+        l = 0u;
+        for (int o = o0; o < o1; ++o)
+            if (oend[o]) {
+                f = min(f, ofirst[o]);
+                l = max(l, oend[o]);
+            }
+    };
+    uint32_t f, l;
+    span(0, 8, f, l);
+    if (l - f <= kTileBlockMax) {
+        emit(f, l);
+        return;
+    }
+    for (int q = 0; q < 4; ++q) {
+        span(2 * q, 2 * q + 2, f, l);
+        if (l <= f) continue;
+        if (l - f <= kTileHalfMax) {
+            emit(f, l);
+        } else {
+            emit(ofirst[2 * q], oend[2 * q]);
+            emit(ofirst[2 * q + 1], oend[2 * q + 1]);
+        }
+    }
+}
+
+// One warp: the density pass of sorted particles p0 .. p0 + 3 of the staged
+// tile (lane group g = lane / 8 takes p0 + g), in lockstep so the warp never
+// runs its groups one after another: the list build is transposed (each lane
+// takes one staged slot of a row and tests it against all four particles), and
+// the sweeps run over the longest of the four lists with the others predicated
+// off.  A particle that the tile path cannot finish is appended to `deferred`
+// (sorted index) with nothing written; k_density_deferred takes it from the
+// start.  The iteration is density_particle's with the neighbour cache never
+// in use (h < MAX_H throughout, so the reference's int max_h stays 0).
+__device__ __forceinline__ void density_tile_warp(const DensityArgs &a, TileShared &S, uint32_t p0, uint32_t end,
+                                                  int lane, uint16_t (*lists)[kTileList], uint32_t *deferred,
+                                                  uint32_t *dctr) {
+    constexpr int L = kTileLanes;
+    constexpr unsigned kFull = 0xffffffffu;
+    constexpr int kBig = 0x3fffffff;
+    const int g = lane / L, sub = lane & (L - 1);
+    uint16_t *list = lists[g];
+    const uint32_t p = p0 + (uint32_t)g;
+    bool live = p < end;  // the group iterates its particle (uniform within the group)
+    uint32_t ind = 0u;
+    float4 me = make_float4(0.f, 0.f, 0.f, 0.f), mv = me;
+    if (live) {
+        ind = a.cidx[p];
+        me = a.sp4[p];
+        mv = a.sv4[p];
+        if (!a.active[ind]) {
+            // density.metal:40-55: EOS only
+            if (sub == 0) {
+                float2 pc = eos_lookup(a.eos, a.mat[ind], a.rho[ind], a.u[ind]);
+                a.P[ind] = pc.x;
+                a.c[ind] = pc.y;
+                float hh = a.h[ind], rho = a.rho[ind], fi = a.f[ind];
+                a.sA[p] = make_float4(me.x, me.y, me.z, hh);
+                a.sB[p] = make_float4(mv.x, mv.y, mv.z, pc.y);
+                a.sC[p] = make_float4(me.w, (fi * pc.x / (rho * rho)), rho, a.B[ind]);
+            }
+            live = false;
+        }
+    }
+    auto defer = [&]() {
+        if (sub == 0) deferred[atomicAdd(dctr, 1u)] = p;
+        live = false;
+    };
+    const float px = me.x, py = me.y, pz = me.z, mi = me.w;
+    float h_plain = 0.5f, hi = 0.5f;
+    bool seeded = false;
+    if (live) {
+        h_plain = a.h[ind];
+        hi = tile_start_h(a, ind, h_plain, seeded);
+        CellBox b;
+        if (S.defer_all || !tile_box(px, py, pz, fmaxf(hi, h_plain), b)) defer();
+    }
+    const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
+    const int ny = S.box[4] - lo1 + 1, nz = S.box[5] - lo2 + 1;
+    // the group's list: staged slots within 2 hb kListReach
+    int n_list = -1;
+    float list_r2 = 0.f;
+    auto build = [&](bool want, float hb) {
+        CellBox b;
+        if (want) {
+            if (!tile_box(px, py, pz, hb, b) || b.lo0 < lo0 || b.lo1 < lo1 || b.lo2 < lo2 || b.hi0 > S.box[3] ||
+                b.hi1 > S.box[4] || b.hi2 > S.box[5]) {
+                defer();
+                want = false;
+            }
+        }
+        if (!want) {
+            b.lo0 = b.lo1 = b.lo2 = kBig;
+            b.hi0 = b.hi1 = b.hi2 = -kBig;
+        }
+        const float rl = 2.f * hb * kListReach;
+        const float r2 = want ? rl * rl : -1.f;
+        const int u0 = __reduce_min_sync(kFull, b.lo0), u1 = __reduce_min_sync(kFull, b.lo1),
+                  u2 = __reduce_min_sync(kFull, b.lo2);
+        const int v0 = __reduce_max_sync(kFull, b.hi0), v1 = __reduce_max_sync(kFull, b.hi1),
+                  v2 = __reduce_max_sync(kFull, b.hi2);
+        if (u0 > v0) return;  // no group builds
+        float qx[4], qy[4], qz[4], qr[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            qx[k] = __shfl_sync(kFull, px, k * L);
+            qy[k] = __shfl_sync(kFull, py, k * L);
+            qz[k] = __shfl_sync(kFull, pz, k * L);
+            qr[k] = __shfl_sync(kFull, r2, k * L);
+        }
+        int cnt[4] = {0, 0, 0, 0};
+        const unsigned below = (1u << lane) - 1u;
+        constexpr float w = kCellWidth;
+        constexpr float iw = 1.f / kCellWidth;
+        // Rows (x, y) of the union box, 32 at a time, one per lane; each row is
+        // trimmed to the z cells that one of the four spheres reaches, and the
+        // trimmed rows are walked as one flat sequence of staged slots, 32
+        // slots per step.
+        const int nyu = v1 - u1 + 1;
+        const int rows = (v0 - u0 + 1) * nyu;
+        for (int rb = 0; rb < rows; rb += 32) {
+            const int r = rb + lane;
+            uint32_t len = 0u, s0 = 0u;
+            if (r < rows) {
+                const int x = u0 + r / nyu, y = u1 + r % nyu;
+                int zl = 0x3fffffff, zh = -0x3fffffff;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float gx = fmaxf(fmaxf((float)x * w - qx[k], qx[k] - (float)(x + 1) * w) - kCellMargin, 0.f);
+                    const float gy = fmaxf(fmaxf((float)y * w - qy[k], qy[k] - (float)(y + 1) * w) - kCellMargin, 0.f);
+                    const float g2 = gx * gx + gy * gy;
+                    if (g2 <= qr[k]) {
+                        const float dz = sqrtf(qr[k] - g2);
+                        zl = min(zl, (int)floorf((qz[k] - dz) * iw - 1e-3f));
+                        zh = max(zh, (int)floorf((qz[k] + dz) * iw + 1e-3f));
+                    }
+                }
+                zl = max(zl, u2);
+                zh = min(zh, v2);
+                if (zl <= zh) {
+                    const int c0 = ((x - lo0) * ny + (y - lo1)) * nz;
+                    s0 = S.off[c0 + (zl - lo2)];
+                    len = S.off[c0 + (zh - lo2) + 1] - s0;
+                }
+            }
+            uint32_t pre = len;  // inclusive scan of the row lengths
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(kFull, pre, o);
+                if (lane >= o) pre += t;
+            }
+            const uint32_t excl = pre - len;
+            const uint32_t total = __shfl_sync(kFull, pre, 31);
+            for (uint32_t vb = 0; vb < total; vb += 32u) {
+                const uint32_t v = vb + (uint32_t)lane;
+                int j = 0;  // the last row whose first flat index is <= v
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const uint32_t e = __shfl_sync(kFull, excl, j + step);
+                    if (e <= v) j += step;
+                }
+                const uint32_t sj = __shfl_sync(kFull, s0, j), ej = __shfl_sync(kFull, excl, j);
+                float4 q = make_float4(3e38f, 3e38f, 3e38f, 0.f);
+                const uint32_t s = sj + (v - ej);
+                if (v < total) q = S.pos[s];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float dx = q.x - qx[k], dy = q.y - qy[k], dz = q.z - qz[k];
+                    const bool hit = dx * dx + dy * dy + dz * dz <= qr[k];
+                    const unsigned bal = __ballot_sync(kFull, hit);
+                    if (hit) {
+                        const int at = cnt[k] + __popc(bal & below);
+                        if (at < kTileList) lists[k][at] = (uint16_t)s;
+                    }
+                    cnt[k] += __popc(bal);
+                }
+            }
+        }
+        __syncwarp();
+        if (want) {
+            const int c = g == 0 ? cnt[0] : g == 1 ? cnt[1] : g == 2 ? cnt[2] : cnt[3];
+            if (c > kTileList) {
+                defer();
+            } else {
+                n_list = c;
+                list_r2 = r2;
+            }
+        }
+    };
+    bool iter = live;
+    bool first = true, fell_back = false;
+    int sweeps = 0, count = 0, nn = 0;
+    float h2x4 = 4.f * hi * hi;
+    float h1 = 1.f / hi;
+    float dens = 0.f, eps = 1.f;
+    float hs = hi, hs2x4 = h2x4;  // the h of the last full sweep
+    while (__any_sync(kFull, iter)) {
+        if (iter) {
+            hs = hi;
+            hs2x4 = h2x4;
+        }
+        const bool want = iter && (n_list < 0 || hs2x4 > list_r2);
+        if (__any_sync(kFull, want)) {
+            build(want, hs);
+            iter = iter && live;
+        }
+        const int maxn = __reduce_max_sync(kFull, iter ? n_list : 0);
+        float part = 0.f;
+        int found = 0;
+#pragma unroll 4
+        for (int i = sub; i < maxn; i += L) {
+            if (iter && i < n_list) {
+                const float4 q = S.pos[list[i]];
+                const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 <= hs2x4) {
+                    const float r = pair_sqrt(r2);
+                    ++found;
+                    part += kernel_w(r, h1) * q.w;
+                }
+            }
+        }
+        const float dsum = group_sum<L>(part, kFull);
+        const int fsum = group_sum_i<L>(found, kFull);
+        if (iter) {
+            dens = dsum;
+            nn = min(fsum, kNeighbourCache);
+            float nh = fmin_ref(kResolutionEta * powf(mi / dens, 1.f / 3), kMaxH);
+            nh = 0.5f * (hi + nh);
+            eps = fabsf(nh - hi) / hi;
+            ++sweeps;
+            if (first && seeded && eps > kSeedFallback) {
+                // the seed disagrees with its own first sweep: start again from
+                // the plain guess
+                first = false;
+                fell_back = true;
+                hi = h_plain;
+                h1 = 1.f / hi;
+                h2x4 = 4.f * hi * hi;
+                nn = 0;
+                eps = 1.f;
+            } else {
+                first = false;
+                if (eps > a.eta) {
+                    if (nh >= kMaxH) {
+                        defer();  // the reference's int max_h would leave 0 from here
+                    } else {
+                        hi = nh;
+                        h1 = 1.f / hi;
+                        h2x4 = 4.f * hi * hi;
+                        count++;
+                    }
+                }
+            }
+            iter = live && eps > a.eta && count < kMaxNR;
+        }
+    }
+    // gradient sweep (density.metal:145-213), as in density_particle
+    const bool gcached = nn < kNeighbourCache;
+    const float g2 = gcached ? hs2x4 : h2x4;
+    const float h2 = hi + hi;
+    {
+        const bool want = live && g2 > list_r2;
+        if (__any_sync(kFull, want)) build(want, gcached ? hs : hi);
+    }
+    const int maxn = __reduce_max_sync(kFull, live ? n_list : 0);
+    const float vix = mv.x, viy = mv.y, viz = mv.z;
+    float pdens = 0.f, dens_h = 0.f, vdiv = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+#pragma unroll 2
+    for (int i = sub; i < maxn; i += L) {
+        if (!(live && i < n_list)) continue;
+        const uint32_t s = list[i];
+        const float4 q = S.pos[s];
+        const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > g2) continue;
+        const float r = pair_sqrt(r2);
+        if (gcached && r > h2) continue;
+        const float mj = q.w;
+        if (!gcached) pdens += kernel_w(r, h1) * mj;
+        dens_h += mj * kernel_dwdh(r, h1);
+        if (r > 1e-12f) {
+            const float r1 = pair_rinv(r2, r);
+            const float4 vj = __ldg(a.sv4 + S.gidx[s]);
+            const float vx = vj.x - vix, vy = vj.y - viy, vz = vj.z - viz;
+            const float sc = kernel_gradw_scale(r, h1);
+            const float gx = sc * (dx * r1), gy = sc * (dy * r1), gz = sc * (dz * r1);
+            vdiv += mj * (vx * gx + vy * gy + vz * gz);
+            cx += mj * (vy * gz - vz * gy);
+            cy += mj * (vz * gx - vx * gz);
+            cz += mj * (vx * gy - vy * gx);
+        }
+    }
+    pdens = group_sum<L>(pdens, kFull);
+    dens_h = group_sum<L>(dens_h, kFull);
+    vdiv = group_sum<L>(vdiv, kFull);
+    cx = group_sum<L>(cx, kFull);
+    cy = group_sum<L>(cy, kFull);
+    cz = group_sum<L>(cz, kFull);
+    if (!live || sub != 0) return;
+    if (!gcached) dens += pdens;
+    if (a.stats) {
+        atomicAdd(&S.stats[0], (uint32_t)sweeps);
+        if (fell_back) atomicAdd(&S.stats[1], 1u);
+        atomicMax(&S.stats[2], (uint32_t)sweeps);
+        atomicAdd(&S.stats[3], 1u);
+    }
+    if (a.nn_out) a.nn_out[ind] = (float)nn;
+    vdiv = fabsf(vdiv) / dens;
+    float acurl = sqrtf(cx * cx + cy * cy + cz * cz) / dens;
+    float fi = 1.f / (1.f + (hi / (3.f * dens)) * dens_h);
+    float2 pc = eos_lookup(a.eos, a.mat[ind], dens, a.u[ind]);
+    float bal = vdiv / (vdiv + acurl + 1e-4f * (pc.y / hi));
+    a.h[ind] = hi;
+    a.rho[ind] = dens;
+    a.f[ind] = fi;
+    a.P[ind] = pc.x;
+    a.c[ind] = pc.y;
+    a.B[ind] = bal;
+    if (!(dens == dens) || !(pc.x == pc.x)) raise_health(a.health, SPH_HEALTH_NAN_DENSITY);
+    a.sA[p] = make_float4(px, py, pz, hi);
+    a.sB[p] = make_float4(vix, viy, viz, pc.y);
+    a.sC[p] = make_float4(mi, (fi * pc.x / (dens * dens)), dens, bal);
+}
+
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_density_tile(DensityArgs a, const uint2 *__restrict__ tiles, uint32_t *ctr, uint32_t *__restrict__ deferred) {
+    extern __shared__ float4 s_tile_raw[];
+    TileShared &S = *reinterpret_cast<TileShared *>(s_tile_raw);
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid < 4) S.stats[tid] = 0u;
+    const uint32_t ntiles = ctr[0];
+    for (;;) {
+        __syncthreads();  // the previous tile is done with the staged data
+        if (tid == 0) {
+            const uint32_t t = atomicAdd(ctr + 1, 1u);
+            S.tile = t;
+            if (t < ntiles) {
+                const uint2 r = tiles[t];
+                S.start = r.x;
+                S.end = r.y;
+            }
+            S.next = 0u;
+            S.box[0] = S.box[1] = S.box[2] = 0x7fffffff;
+            S.box[3] = S.box[4] = S.box[5] = -0x7fffffff;
+            S.defer_all = 0;
+        }
+        __syncthreads();
+        if (S.tile >= ntiles) break;
+        const uint32_t start = S.start, end = S.end;
+        // the staged box: union of the list boxes of the tile's active particles
+        {
+            int b[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, -0x7fffffff, -0x7fffffff, -0x7fffffff};
+            for (uint32_t p = start + tid; p < end; p += kTileThreads) {
+                const uint32_t ind = a.cidx[p];
+                if (!a.active[ind]) continue;
+                const float4 me = a.sp4[p];
+                const float h_plain = a.h[ind];
+                bool seeded;
+                const float h0 = tile_start_h(a, ind, h_plain, seeded);
+                CellBox cb;
+                if (!tile_box(me.x, me.y, me.z, fmaxf(h0, h_plain), cb)) continue;
+                b[0] = min(b[0], cb.lo0);
+                b[1] = min(b[1], cb.lo1);
+                b[2] = min(b[2], cb.lo2);
+                b[3] = max(b[3], cb.hi0);
+                b[4] = max(b[4], cb.hi1);
+                b[5] = max(b[5], cb.hi2);
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                b[k] = __reduce_min_sync(0xffffffffu, b[k]);
+                b[k + 3] = __reduce_max_sync(0xffffffffu, b[k + 3]);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    atomicMin(&S.box[k], b[k]);
+                    atomicMax(&S.box[k + 3], b[k + 3]);
+                }
+            }
+        }
+        __syncthreads();
+        const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
+        const bool any = lo0 <= S.box[3];  // some particle of the tile takes the tile path
+        const int nx = any ? S.box[3] - lo0 + 1 : 0, ny = any ? S.box[4] - lo1 + 1 : 0,
+                  nz = any ? S.box[5] - lo2 + 1 : 0;
+        int ncell = 0;
+        if (any) {
+            if (nx * ny * nz > kTileCellsMax) {
+                if (tid == 0) S.defer_all = 1;
+            } else {
+                ncell = nx * ny * nz;
+            }
+        }
+        // cell counts (kTileCellsPerThread consecutive cells per thread) and
+        // their exclusive scan
+        uint32_t c_cnt[kTileCellsPerThread];
+        uint32_t tsum = 0u;
+#pragma unroll
+        for (int k = 0; k < kTileCellsPerThread; ++k) {
+            const int c = kTileCellsPerThread * tid + k;
+            c_cnt[k] = 0u;
+            if (c < ncell) {
+                const int ix = c / (ny * nz), rem = c - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
+                const uint2 r = __ldg(a.cells + cell_index_of(lo0 + ix, lo1 + iy, lo2 + iz));
+                if (r.x != 0xffffffffu) {
+                    c_cnt[k] = r.y - r.x + 1u;
+                    S.first[c] = r.x;
+                }
+            }
+            tsum += c_cnt[k];
+        }
+        uint32_t inc = tsum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) S.wsum[tid >> 5] = inc;
+        __syncthreads();
+        uint32_t wbase = 0u;
+        for (int w = 0; w < (tid >> 5); ++w) wbase += S.wsum[w];
+        uint32_t run = wbase + inc - tsum;
+#pragma unroll
+        for (int k = 0; k < kTileCellsPerThread; ++k) {
+            const int c = kTileCellsPerThread * tid + k;
+            if (c < ncell) S.off[c] = run;
+            run += c_cnt[k];
+        }
+        if (tid == kTileThreads - 1) {
+            S.off[ncell] = run;
+            if (run > (uint32_t)kTileStageMax) S.defer_all = 1;
+        }
+        __syncthreads();
+        if (!S.defer_all) {
+            const uint32_t total = S.off[ncell];
+            for (uint32_t s = tid; s < total; s += kTileThreads) {
+                int lo = 0, hi = ncell - 1;  // the last cell whose first slot is <= s
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S.off[mid] <= s) lo = mid;
+                    else hi = mid - 1;
+                }
+                const uint32_t g = S.first[lo] + (s - S.off[lo]);
+                S.pos[s] = __ldg(a.sp4 + g);
+                S.gidx[s] = g;
+            }
+        }
+        __syncthreads();
+        // warps take the tile's particles four at a time
+        for (;;) {
+            uint32_t j = 0u;
+            if (lane == 0) j = atomicAdd(&S.next, 4u);
+            j = __shfl_sync(0xffffffffu, j, 0);
+            if (start + j >= end) break;
+            density_tile_warp(a, S, start + j, end, lane, &S.list[(tid >> 5) * 4], deferred, ctr + 2);
+        }
+    }
+    if (a.stats && tid == 0) {
+        if (S.stats[3]) {
+            atomicAdd(a.stats + 0, S.stats[0]);
+            if (S.stats[1]) atomicAdd(a.stats + 1, S.stats[1]);
+            atomicMax(a.stats + 2, S.stats[2]);
+            atomicAdd(a.stats + 3, S.stats[3]);
+        }
+    }
 }
 
 struct AccelArgs {
@@ -804,6 +1417,22 @@ size_t list_smem_opt_in() {
     return smem;
 }
 
+// Shared memory of the tile kernel (above 48 KiB: the per-device opt-in) and
+// the device's SM count, set up once per device.
+int tile_smem_opt_in() {
+    static int sms[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!sms[dev]) {
+        cudaFuncSetAttribute(k_density_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileShared));
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        sms[dev] = v > 0 ? v : 148;
+    }
+    return sms[dev];
+}
+
 }  // namespace
 
 sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
@@ -848,7 +1477,18 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     a.stats = ctx->hs.stats;
     constexpr int parts = parts_per_block<kLanesPerParticle>();
     const size_t smem = list_smem_opt_in();
+#ifdef SPH_PARITY
+    // one lane per particle, in the reference's order
     k_density<kLanesPerParticle><<<(unsigned)((n + parts - 1) / parts), parts * kLanesPerParticle, smem, st>>>(a);
+#else
+    const int sms = tile_smem_opt_in();
+    cudaMemsetAsync(ctx->tile_ctr, 0, sizeof(uint32_t) * 4, st);
+    k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->cell_sort.keys[ctx->cell_final], ctx->cell_range,
+                                                   ctx->tiles, ctx->tile_ctr, ctx->globals);
+    k_density_tile<<<sms * 2, kTileThreads, sizeof(TileShared), st>>>(a, ctx->tiles, ctx->tile_ctr, ctx->deferred);
+    k_density_deferred<kLanesPerParticle><<<sms * 8, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred,
+                                                                                           ctx->tile_ctr + 2);
+#endif
     if (ctx->hs.capture) s = launch_hseed_targets(ctx, st);
     if (s != SPH_OK) return s;
     return cuda_status(cudaGetLastError(), "density");
