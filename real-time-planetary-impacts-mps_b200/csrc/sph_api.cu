@@ -383,7 +383,7 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     chk(dmalloc(&ctx->dglob, 4));
     chk(dmalloc(&ctx->diag, (size_t)kDiagDoubles));
     chk(dmalloc(&ctx->tiles, (size_t)n));
-    chk(dmalloc(&ctx->tile_ctr, 4));
+    chk(dmalloc(&ctx->tile_ctr, 8));
     chk(dmalloc(&ctx->deferred, (size_t)n));
     if (e != cudaSuccess) {
         s = cuda_status(e, "sph_create allocation");

@@ -618,7 +618,7 @@ __device__ __forceinline__ float tile_start_h(const DensityArgs &a, uint32_t ind
 __global__ void k_tile_starts(int n, const uint32_t *__restrict__ skey, const uint2 *__restrict__ cells,
                               uint2 *__restrict__ tiles, uint32_t *ctr, int32_t *globals) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0) globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
+    if (k == 0 && globals) globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
     if (k >= n) return;
     const uint32_t blk = skey[k] >> 6;
     if (k > 0 && (skey[k - 1] >> 6) == blk) return;
@@ -1122,139 +1122,549 @@ struct AccelArgs {
     int32_t *globals;
 };
 
+// The particle's own terms of accelerations.metal:60-141.
+struct AccelI {
+    float xi, yi, zi, hi, vxi, vyi, vzi, ci, facti, rhoi, Bi, hi1, hi2x4;
+};
+__device__ __forceinline__ AccelI accel_i(const float4 A, const float4 Bv, const float4 Cv) {
+    AccelI I;
+    I.xi = A.x;
+    I.yi = A.y;
+    I.zi = A.z;
+    I.hi = A.w;
+    I.vxi = Bv.x;
+    I.vyi = Bv.y;
+    I.vzi = Bv.z;
+    I.ci = Bv.w;
+    I.facti = Cv.y;
+    I.rhoi = Cv.z;
+    I.Bi = Cv.w;
+    I.hi1 = 1.f / I.hi;
+    I.hi2x4 = I.hi * I.hi * 4.f;
+    return I;
+}
+// Running sums of one particle (a slice of its pairs): acceleration, du/dt,
+// dh/dt, with Kahan compensations in the mixed-precision form, and the
+// largest signal speed.
+struct AccelSum {
+    float dvx = 0.f, dvy = 0.f, dvz = 0.f, du = 0.f, dh = 0.f;
+    float kx = 0.f, ky = 0.f, kz = 0.f, ku = 0.f, kh = 0.f;
+    float vsig = 1e-12f;
+};
+template <bool KAHAN>
+__device__ __forceinline__ void accel_add(float &sum, float &comp, float v) {
+    if (KAHAN) {
+        const float y = v - comp;
+        const float t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    } else {
+        sum += v;
+    }
+}
+// accelerations.metal:75-124: one accepted pair (Aj = (x, y, z, h),
+// Bj = (v, c), Cj = (m, f P / rho^2, rho, B) of the neighbour).
+template <bool KAHAN>
+__device__ __forceinline__ void accel_pair(const AccelI &I, AccelSum &S, const float4 Aj, const float4 Bj,
+                                           const float4 Cj) {
+    const float dx = I.xi - Aj.x, dy = I.yi - Aj.y, dz = I.zi - Aj.z;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float hj = Aj.w;
+    const float r = pair_sqrt(r2);
+    const float r1 = pair_rinv(r2, r);
+    const float mj = Cj.x, factj = Cj.y, rhoj = Cj.z, Balj = Cj.w;
+    const float hj1 = 1.f / hj;
+    const float vx = I.vxi - Bj.x, vy = I.vyi - Bj.y, vz = I.vzi - Bj.z;
+    const float rhoij = 0.5f * (I.rhoi + rhoj);
+    const float vdr = vx * dx + vy * dy + vz * dz;
+    const float mu = vdr < 0.f ? vdr * r1 : 0.f;
+    const float vsig = I.ci + Bj.w - 3.f * mu;
+    S.vsig = fmax_ref(vsig, S.vsig);
+    const float Bij = 0.5f * (I.Bi + Balj);
+    const float nu = -0.5f * kViscosityAlpha * Bij * mu * vsig / rhoij;
+    const float rhx = dx * r1, rhy = dy * r1, rhz = dz * r1;
+    const float si = kernel_gradw_scale(r, I.hi1), sj = kernel_gradw_scale(r, hj1);
+    const float gix = si * rhx, giy = si * rhy, giz = si * rhz;
+    const float gjx = sj * rhx, gjy = sj * rhy, gjz = sj * rhz;
+    const float gx = 0.5f * (gix + gjx), gy = 0.5f * (giy + gjy), gz = 0.5f * (giz + gjz);
+    accel_add<KAHAN>(S.dvx, S.kx, -(mj * (I.facti * gix + factj * gjx + nu * gx)));
+    accel_add<KAHAN>(S.dvy, S.ky, -(mj * (I.facti * giy + factj * gjy + nu * gy)));
+    accel_add<KAHAN>(S.dvz, S.kz, -(mj * (I.facti * giz + factj * gjz + nu * gz)));
+    accel_add<KAHAN>(S.du, S.ku,
+                     mj * (I.facti * (vx * gix + vy * giy + vz * giz) + 0.5f * nu * (vx * gx + vy * gy + vz * gz)));
+    accel_add<KAHAN>(S.dh, S.kh, (mj / rhoj) * (vx * gix + vy * giy + vz * giz));
+}
+// The group's sums combined (every lane ends with the same bits).
+template <int L, bool KAHAN>
+__device__ __forceinline__ void accel_reduce(AccelSum &S, unsigned gm) {
+    if (KAHAN) {
+        S.dvx -= S.kx;
+        S.dvy -= S.ky;
+        S.dvz -= S.kz;
+        S.du -= S.ku;
+        S.dh -= S.kh;
+    }
+    S.dvx = group_sum<L>(S.dvx, gm);
+    S.dvy = group_sum<L>(S.dvy, gm);
+    S.dvz = group_sum<L>(S.dvz, gm);
+    S.du = group_sum<L>(S.du, gm);
+    S.dh = group_sum<L>(S.dh, gm);
+    S.vsig = group_max<L>(S.vsig, gm);
+}
+// accelerations.metal:129-140: the particle's timestep in ticks.
+__device__ __forceinline__ int accel_ticks(const AccelI &I, float vsig) {
+    const float goal = 2.0f * kCFL * kGamma * I.hi / vsig;
+    int r = 0;
+    float cand = kDT0;
+    while (cand > goal && r < kRMax) {
+        cand *= 0.5f;
+        r++;
+    }
+    return (int)ceilf(1 / kDtMin1 * cand);
+}
+__device__ __forceinline__ void accel_store(const AccelArgs &a, uint32_t ind, const AccelSum &S, int idt) {
+    float4 acc = a.acc4[ind];
+    acc.x += S.dvx;
+    acc.y += S.dvy;
+    acc.z += S.dvz;
+    a.acc4[ind] = acc;
+    a.du[ind] = S.du;
+    a.dhdt[ind] = S.dh;
+    a.nat[ind] = a.globals[0] + idt;
+}
+
 // accelerations.metal:12-141 for one sorted particle per lane group.  The
 // walk covers the particle's own box of radius 2 min(h, MAX_SMOOTHING_LENGTH)
 // (the reference's box, which also decides which pairs with r < 2 h_j are
 // seen, Q8).  The pairs that pass the reference's test are first collected in
 // order into the group's list, then evaluated by all lanes of the group
-// together, so the long pair computation runs with every lane busy.
+// together, so the long pair computation runs with every lane busy.  Returns
+// the particle's timestep in ticks (INT_MAX when inactive).
 template <int L, bool KAHAN>
-__global__ void __launch_bounds__(parts_per_block<L>() * L) k_acceleration(AccelArgs a) {
-    extern __shared__ uint32_t s_lists[];
-    __shared__ uint32_t s_off[parts_per_block<L>() * L], s_start[parts_per_block<L>() * L];
-    __shared__ int wmin[32];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31, sub = lane & (L - 1), gbase = lane & ~(L - 1);
-    uint32_t *w_off = s_off + (threadIdx.x & ~31), *w_start = s_start + (threadIdx.x & ~31);
-    uint32_t *list = s_lists + (size_t)(threadIdx.x / L) * kListMax;
-    const unsigned gm = group_mask<L>(lane);
-    const int index = t / L;
-    int idt = 0x7fffffff;
-    if (index < a.n) {
-        const uint32_t ind = a.cidx[index];
-        if (a.active[ind]) {
-            const float4 A = a.sA[index], Bv = a.sB[index], Cv = a.sC[index];
-            const float xi = A.x, yi = A.y, zi = A.z, hi = A.w;
-            const float vxi = Bv.x, vyi = Bv.y, vzi = Bv.z, ci = Bv.w;
-            const float facti = Cv.y, rhoi = Cv.z, Bi = Cv.w;
-            const float hi1 = 1.f / hi;
-            const float hi2x4 = hi * hi * 4.f;
-            float dvx = 0.f, dvy = 0.f, dvz = 0.f, du = 0.f, dh = 0.f;
-            // compensations of the Kahan sums (mixed-precision form)
-            float kx = 0.f, ky = 0.f, kz = 0.f, ku = 0.f, kh = 0.f;
-            float vsig_i = 1e-12f;
-            const float4 *sA = a.sA, *sB = a.sB, *sC = a.sC;
-            auto add = [&](float &sum, float &comp, float v) {
-                if (KAHAN) {
-                    const float y = v - comp;
-                    const float t = sum + y;
-                    comp = (t - sum) - y;
-                    sum = t;
-                } else {
-                    sum += v;
-                }
-            };
-            auto pair = [&](uint32_t k) {
-                const float4 Aj = __ldg(sA + k);
-                const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                const float hj = Aj.w;
-                const float4 Cj = __ldg(sC + k);
-                const float4 Bj = __ldg(sB + k);
-                const float r = pair_sqrt(r2);
-                const float r1 = 1.f / r;
-                const float mj = Cj.x, factj = Cj.y, rhoj = Cj.z, Balj = Cj.w;
-                const float hj1 = 1.f / hj;
-                const float vx = vxi - Bj.x, vy = vyi - Bj.y, vz = vzi - Bj.z;
-                const float rhoij = 0.5f * (rhoi + rhoj);
-                const float vdr = vx * dx + vy * dy + vz * dz;
-                const float mu = vdr < 0.f ? vdr * r1 : 0.f;
-                const float vsig = ci + Bj.w - 3.f * mu;
-                vsig_i = fmax_ref(vsig, vsig_i);
-                const float Bij = 0.5f * (Bi + Balj);
-                const float nu = -0.5f * kViscosityAlpha * Bij * mu * vsig / rhoij;
-                const float rhx = dx * r1, rhy = dy * r1, rhz = dz * r1;
-                const float si = kernel_gradw_scale(r, hi1), sj = kernel_gradw_scale(r, hj1);
-                const float gix = si * rhx, giy = si * rhy, giz = si * rhz;
-                const float gjx = sj * rhx, gjy = sj * rhy, gjz = sj * rhz;
-                const float gx = 0.5f * (gix + gjx), gy = 0.5f * (giy + gjy), gz = 0.5f * (giz + gjz);
-                add(dvx, kx, -(mj * (facti * gix + factj * gjx + nu * gx)));
-                add(dvy, ky, -(mj * (facti * giy + factj * gjy + nu * gy)));
-                add(dvz, kz, -(mj * (facti * giz + factj * gjz + nu * gz)));
-                add(du, ku, mj * (facti * (vx * gix + vy * giy + vz * giz) + 0.5f * nu * (vx * gx + vy * gy + vz * gz)));
-                add(dh, kh, (mj / rhoj) * (vx * gix + vy * giy + vz * giz));
-            };
-            auto drain = [&](int cnt) {
-                __syncwarp(gm);
-                for (int i = sub; i < cnt; i += L) pair(list[i]);
-                __syncwarp(gm);
-                return true;
-            };
-            const int rest = group_collect<L>(
-                xi, yi, zi, fmin_ref(hi, kMaxH), 3.402823466e+38f, a.cells, sub, gm, gbase, w_off, w_start, list,
-                kListMax,
-                [&](uint32_t k) {
-                    const float4 Aj = __ldg(sA + k);
-                    const float dx = xi - Aj.x, dy = yi - Aj.y, dz = zi - Aj.z;
-                    const float r2 = dx * dx + dy * dy + dz * dz;
-                    const float hj2x4 = Aj.w * Aj.w * 4.f;
-                    return !((r2 > hi2x4 && r2 > hj2x4) || r2 < 1e-12f);
-                },
-                drain);
-            drain(rest);
-            if (KAHAN) {
-                dvx -= kx;
-                dvy -= ky;
-                dvz -= kz;
-                du -= ku;
-                dh -= kh;
-            }
-            dvx = group_sum<L>(dvx, gm);
-            dvy = group_sum<L>(dvy, gm);
-            dvz = group_sum<L>(dvz, gm);
-            du = group_sum<L>(du, gm);
-            dh = group_sum<L>(dh, gm);
-            vsig_i = group_max<L>(vsig_i, gm);
-            // accelerations.metal:129-140
-            const float goal = 2.0f * kCFL * kGamma * hi / vsig_i;
-            int r = 0;
-            float cand = kDT0;
-            while (cand > goal && r < kRMax) {
-                cand *= 0.5f;
-                r++;
-            }
-            idt = (int)ceilf(1 / kDtMin1 * cand);
-            if (sub == 0) {
-                float4 acc = a.acc4[ind];
-                acc.x += dvx;
-                acc.y += dvy;
-                acc.z += dvz;
-                a.acc4[ind] = acc;
-                a.du[ind] = du;
-                a.dhdt[ind] = dh;
-                a.nat[ind] = a.globals[0] + idt;
-            }
+__device__ __forceinline__ int accel_particle(const AccelArgs &a, int index, int sub, unsigned gm, int gbase,
+                                              uint32_t *w_off, uint32_t *w_start, uint32_t *list) {
+    const uint32_t ind = a.cidx[index];
+    if (!a.active[ind]) return 0x7fffffff;
+    const AccelI I = accel_i(a.sA[index], a.sB[index], a.sC[index]);
+    AccelSum S;
+    const float4 *sA = a.sA, *sB = a.sB, *sC = a.sC;
+    auto drain = [&](int cnt) {
+        __syncwarp(gm);
+        for (int i = sub; i < cnt; i += L) {
+            const uint32_t k = list[i];
+            accel_pair<KAHAN>(I, S, __ldg(sA + k), __ldg(sB + k), __ldg(sC + k));
         }
-    }
-    // block-wide minimum, then one atomic per block
+        __syncwarp(gm);
+        return true;
+    };
+    const int rest = group_collect<L>(
+        I.xi, I.yi, I.zi, fmin_ref(I.hi, kMaxH), 3.402823466e+38f, a.cells, sub, gm, gbase, w_off, w_start, list,
+        kListMax,
+        [&](uint32_t k) {
+            const float4 Aj = __ldg(sA + k);
+            const float dx = I.xi - Aj.x, dy = I.yi - Aj.y, dz = I.zi - Aj.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            const float hj2x4 = Aj.w * Aj.w * 4.f;
+            return !((r2 > I.hi2x4 && r2 > hj2x4) || r2 < 1e-12f);
+        },
+        drain);
+    drain(rest);
+    accel_reduce<L, KAHAN>(S, gm);
+    const int idt = accel_ticks(I, S.vsig);
+    if (sub == 0) accel_store(a, ind, S, idt);
+    return idt;
+}
+
+// Block-wide minimum of the timesteps, then one atomic per block.
+__device__ __forceinline__ void block_min_dt(int idt, int32_t *dt) {
+    __shared__ int wmin[32];
+    const int lane = threadIdx.x & 31;
     for (int o = 16; o > 0; o >>= 1) idt = min(idt, __shfl_xor_sync(0xffffffffu, idt, o));
     if (lane == 0) wmin[threadIdx.x >> 5] = idt;
     __syncthreads();
     if (threadIdx.x < 32) {
         int v = (threadIdx.x < ((blockDim.x + 31) >> 5)) ? wmin[threadIdx.x] : 0x7fffffff;
         for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (threadIdx.x == 0 && v != 0x7fffffff) atomicMin(&a.globals[1], v);
+        if (threadIdx.x == 0 && v != 0x7fffffff) atomicMin(dt, v);
     }
+}
+
+template <int L, bool KAHAN>
+__global__ void __launch_bounds__(parts_per_block<L>() * L) k_acceleration(AccelArgs a) {
+    extern __shared__ uint32_t s_lists[];
+    __shared__ uint32_t s_off[parts_per_block<L>() * L], s_start[parts_per_block<L>() * L];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, sub = lane & (L - 1), gbase = lane & ~(L - 1);
+    const int index = t / L;
+    int idt = 0x7fffffff;
+    if (index < a.n)
+        idt = accel_particle<L, KAHAN>(a, index, sub, group_mask<L>(lane), gbase, s_off + (threadIdx.x & ~31),
+                                       s_start + (threadIdx.x & ~31),
+                                       s_lists + (size_t)(threadIdx.x / L) * kListMax);
+    block_min_dt(idt, a.globals + 1);
+}
+
+// The particles the tile pass handed on (sorted indices idx[0, *count)).
+template <int L, bool KAHAN>
+__global__ void __launch_bounds__(parts_per_block<L>() * L)
+    k_acceleration_deferred(AccelArgs a, const uint32_t *__restrict__ idx, const uint32_t *__restrict__ count) {
+    extern __shared__ uint32_t s_lists[];
+    __shared__ uint32_t s_off[parts_per_block<L>() * L], s_start[parts_per_block<L>() * L];
+    const int lane = threadIdx.x & 31, sub = lane & (L - 1), gbase = lane & ~(L - 1);
+    const uint32_t cnt = *count;
+    constexpr int per_block = parts_per_block<L>();
+    int idt = 0x7fffffff;
+    for (uint32_t base = blockIdx.x * per_block; base < cnt; base += gridDim.x * per_block) {
+        const uint32_t j = base + threadIdx.x / L;
+        if (j < cnt)
+            idt = min(idt, accel_particle<L, KAHAN>(a, (int)idx[j], sub, group_mask<L>(lane), gbase,
+                                                    s_off + (threadIdx.x & ~31), s_start + (threadIdx.x & ~31),
+                                                    s_lists + (size_t)(threadIdx.x / L) * kListMax));
+    }
+    block_min_dt(idt, a.globals + 1);
+}
+
+// ---- acceleration over cell tiles (product build) ---------------------------
+//
+// The tiles of the density pass (k_tile_starts), staged the same way with the
+// sA records (x, y, z, h) of the union of the tile particles' boxes of radius
+// 2 min(h, MAX_H) -- the reference's box, exact (cell_box) -- plus each staged
+// particle's cell within the staged box.  Warps take four particles at a time:
+// the transposed list build walks the rows of the four boxes as one flat
+// sequence and keeps a pair when r <= 2 h_i, or when r <= 2 h_j and the
+// neighbour's cell lies in the particle's box (the reference sees such a pair
+// only there, Q8); then the pair arithmetic runs over the lists with every
+// lane busy, reading the neighbour's sB / sC records by its sorted index.
+// Particles whose box reaches more than kTileReach cells past their own cell,
+// whose list overflows, and every particle of a tile whose staged box exceeds
+// the budget go to k_acceleration_deferred.
+constexpr int kTileAccStage = 3072;  // staged particles per tile
+
+struct TileAccShared {
+    float4 pos[kTileAccStage];          // staged sA (x, y, z, h)
+    uint32_t gidx[kTileAccStage];       // staged sorted index
+    uint32_t scell[kTileAccStage];      // staged cell, box-relative: x | y << 10 | z << 20
+    uint32_t off[kTileCellsMax + 1];
+    uint32_t first[kTileCellsMax];
+    uint16_t list[kTileGroups][kTileList];
+    int gbox[kTileGroups][6];           // each group's box, box-relative lo xyz, hi xyz
+    int box[6];
+    uint32_t wsum[kTileThreads / 32];
+    uint32_t start, end, tile, next;
+    int defer_all;
+    int dtmin;
+};
+
+// The reference's box of an acceleration particle and whether the tile path
+// can take it (reach within kTileReach cells of its own, h < MAX_H).
+__device__ __forceinline__ bool accel_box(float px, float py, float pz, float h, CellBox &b) {
+    b = cell_box(px, py, pz, fmin_ref(h, kMaxH));
+    const int ox = (int)floorf(__fdiv_rn(px, kCellWidth)), oy = (int)floorf(__fdiv_rn(py, kCellWidth)),
+              oz = (int)floorf(__fdiv_rn(pz, kCellWidth));
+    return h < kMaxH && ox - b.lo0 <= kTileReach && b.hi0 - ox <= kTileReach && oy - b.lo1 <= kTileReach &&
+           b.hi1 - oy <= kTileReach && oz - b.lo2 <= kTileReach && b.hi2 - oz <= kTileReach;
+}
+
+// One warp: the acceleration pass of sorted particles p0 .. p0 + 3 of the
+// staged tile (lane group g takes p0 + g).  Returns the warp's smallest
+// timestep in ticks (INT_MAX when none).
+template <bool KAHAN>
+__device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared &S, uint32_t p0, uint32_t end,
+                                               int lane, int wslot, uint32_t *deferred, uint32_t *dctr) {
+    constexpr int L = kTileLanes;
+    constexpr unsigned kFull = 0xffffffffu;
+    constexpr int kBig = 0x3fffffff;
+    const int g = lane / L, sub = lane & (L - 1);
+    uint16_t *list = S.list[wslot * 4 + g];
+    const uint32_t p = p0 + (uint32_t)g;
+    bool live = p < end;
+    uint32_t ind = 0u;
+    if (live) {
+        ind = a.cidx[p];
+        live = a.active[ind] != 0;
+    }
+    float4 A = make_float4(0.f, 0.f, 0.f, 1.f), Bv = A, Cv = A;
+    if (live) {
+        A = a.sA[p];
+        Bv = a.sB[p];
+        Cv = a.sC[p];
+    }
+    const AccelI I = accel_i(A, Bv, Cv);
+    const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
+    const int ny = S.box[4] - lo1 + 1, nz = S.box[5] - lo2 + 1;
+    CellBox b;
+    bool want = false;
+    if (live) {
+        if (S.defer_all || !accel_box(I.xi, I.yi, I.zi, I.hi, b)) {
+            if (sub == 0) deferred[atomicAdd(dctr, 1u)] = p;
+            live = false;
+        } else {
+            want = true;
+        }
+    }
+    if (!want) {
+        b.lo0 = b.lo1 = b.lo2 = kBig;
+        b.hi0 = b.hi1 = b.hi2 = -kBig;
+    }
+    if (want && sub == 0) {
+        int *gb = S.gbox[wslot * 4 + g];
+        gb[0] = b.lo0 - lo0;
+        gb[1] = b.lo1 - lo1;
+        gb[2] = b.lo2 - lo2;
+        gb[3] = b.hi0 - lo0;
+        gb[4] = b.hi1 - lo1;
+        gb[5] = b.hi2 - lo2;
+    }
+    const int u0 = __reduce_min_sync(kFull, b.lo0), u1 = __reduce_min_sync(kFull, b.lo1),
+              u2 = __reduce_min_sync(kFull, b.lo2);
+    const int v0 = __reduce_max_sync(kFull, b.hi0), v1 = __reduce_max_sync(kFull, b.hi1),
+              v2 = __reduce_max_sync(kFull, b.hi2);
+    if (u0 > v0) return 0x7fffffff;  // no active particle takes the tile path
+    __syncwarp();
+    float qx[4], qy[4], qz[4], qr[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        qx[k] = __shfl_sync(kFull, I.xi, k * L);
+        qy[k] = __shfl_sync(kFull, I.yi, k * L);
+        qz[k] = __shfl_sync(kFull, I.zi, k * L);
+        qr[k] = __shfl_sync(kFull, want ? I.hi2x4 : -1.f, k * L);
+    }
+    // box bounds of the four groups, for the row test (lane k * L holds group k's)
+    int cnt[4] = {0, 0, 0, 0};
+    const unsigned below = (1u << lane) - 1u;
+    const int nyu = v1 - u1 + 1;
+    const int rows = (v0 - u0 + 1) * nyu;
+    for (int rb = 0; rb < rows; rb += 32) {
+        const int r = rb + lane;
+        uint32_t len = 0u, s0 = 0u;
+        int zl = kBig, zh = -kBig;
+        int x = 0, y = 0;
+        if (r < rows) {
+            x = u0 + r / nyu;
+            y = u1 + r % nyu;
+        }
+        // the z range of the boxes that contain row (x, y)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int bl0 = __shfl_sync(kFull, b.lo0, k * L), bh0 = __shfl_sync(kFull, b.hi0, k * L);
+            const int bl1 = __shfl_sync(kFull, b.lo1, k * L), bh1 = __shfl_sync(kFull, b.hi1, k * L);
+            const int bl2 = __shfl_sync(kFull, b.lo2, k * L), bh2 = __shfl_sync(kFull, b.hi2, k * L);
+            if (r < rows && x >= bl0 && x <= bh0 && y >= bl1 && y <= bh1) {
+                zl = min(zl, bl2);
+                zh = max(zh, bh2);
+            }
+        }
+        if (zl <= zh) {
+            const int c0 = ((x - lo0) * ny + (y - lo1)) * nz;
+            s0 = S.off[c0 + (zl - lo2)];
+            len = S.off[c0 + (zh - lo2) + 1] - s0;
+        }
+        uint32_t pre = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFull, pre, o);
+            if (lane >= o) pre += t;
+        }
+        const uint32_t excl = pre - len;
+        const uint32_t total = __shfl_sync(kFull, pre, 31);
+        for (uint32_t vb = 0; vb < total; vb += 32u) {
+            const uint32_t v = vb + (uint32_t)lane;
+            int j = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const uint32_t e = __shfl_sync(kFull, excl, j + step);
+                if (e <= v) j += step;
+            }
+            const uint32_t sj = __shfl_sync(kFull, s0, j), ej = __shfl_sync(kFull, excl, j);
+            const uint32_t s = sj + (v - ej);
+            float4 q = make_float4(3e38f, 3e38f, 3e38f, 0.f);
+            uint32_t sc = 0u;
+            if (v < total) {
+                q = S.pos[s];
+                sc = S.scell[s];
+            }
+            const float hj2x4 = q.w * q.w * 4.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float dx = qx[k] - q.x, dy = qy[k] - q.y, dz = qz[k] - q.z;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const bool near = r2 >= 1e-12f;
+                bool hit = near && r2 <= qr[k];
+                // r > 2 h_i but r <= 2 h_j: only when the neighbour's cell is in the box
+                const bool maybe = near && !hit && qr[k] >= 0.f && r2 <= hj2x4;
+                if (__any_sync(kFull, maybe)) {
+                    const int *gb = S.gbox[wslot * 4 + k];
+                    const int cx = (int)(sc & 1023u), cy = (int)((sc >> 10) & 1023u), cz = (int)(sc >> 20);
+                    if (maybe && cx >= gb[0] && cx <= gb[3] && cy >= gb[1] && cy <= gb[4] && cz >= gb[2] &&
+                        cz <= gb[5])
+                        hit = true;
+                }
+                const unsigned bal = __ballot_sync(kFull, hit);
+                if (hit) {
+                    const int at = cnt[k] + __popc(bal & below);
+                    if (at < kTileList) S.list[wslot * 4 + k][at] = (uint16_t)s;
+                }
+                cnt[k] += __popc(bal);
+            }
+        }
+    }
+    __syncwarp();
+    const int n_list = g == 0 ? cnt[0] : g == 1 ? cnt[1] : g == 2 ? cnt[2] : cnt[3];
+    if (live && n_list > kTileList) {
+        if (sub == 0) deferred[atomicAdd(dctr, 1u)] = p;
+        live = false;
+    }
+    const int maxn = __reduce_max_sync(kFull, live ? n_list : 0);
+    AccelSum Sm;
+#pragma unroll 2
+    for (int i = sub; i < maxn; i += L) {
+        if (live && i < n_list) {
+            const uint32_t s = list[i];
+            const uint32_t gj = S.gidx[s];
+            accel_pair<KAHAN>(I, Sm, S.pos[s], __ldg(a.sB + gj), __ldg(a.sC + gj));
+        }
+    }
+    accel_reduce<L, KAHAN>(Sm, kFull);
+    int idt = 0x7fffffff;
+    if (live) {
+        idt = accel_ticks(I, Sm.vsig);
+        if (sub == 0) accel_store(a, ind, Sm, idt);
+    }
+    return __reduce_min_sync(kFull, idt);
+}
+
+template <bool KAHAN>
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_acceleration_tile(AccelArgs a, const uint2 *__restrict__ tiles, uint32_t *ctr, uint32_t *__restrict__ deferred) {
+    extern __shared__ float4 s_tile_raw[];
+    TileAccShared &S = *reinterpret_cast<TileAccShared *>(s_tile_raw);
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid == 0) S.dtmin = 0x7fffffff;
+    const uint32_t ntiles = ctr[0];
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t t = atomicAdd(ctr + 1, 1u);
+            S.tile = t;
+            if (t < ntiles) {
+                const uint2 r = tiles[t];
+                S.start = r.x;
+                S.end = r.y;
+            }
+            S.next = 0u;
+            S.box[0] = S.box[1] = S.box[2] = 0x7fffffff;
+            S.box[3] = S.box[4] = S.box[5] = -0x7fffffff;
+            S.defer_all = 0;
+        }
+        __syncthreads();
+        if (S.tile >= ntiles) break;
+        const uint32_t start = S.start, end = S.end;
+        {
+            int b[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, -0x7fffffff, -0x7fffffff, -0x7fffffff};
+            for (uint32_t p = start + tid; p < end; p += kTileThreads) {
+                if (!a.active[a.cidx[p]]) continue;
+                const float4 A = a.sA[p];
+                CellBox cb;
+                if (!accel_box(A.x, A.y, A.z, A.w, cb)) continue;
+                b[0] = min(b[0], cb.lo0);
+                b[1] = min(b[1], cb.lo1);
+                b[2] = min(b[2], cb.lo2);
+                b[3] = max(b[3], cb.hi0);
+                b[4] = max(b[4], cb.hi1);
+                b[5] = max(b[5], cb.hi2);
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                b[k] = __reduce_min_sync(0xffffffffu, b[k]);
+                b[k + 3] = __reduce_max_sync(0xffffffffu, b[k + 3]);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    atomicMin(&S.box[k], b[k]);
+                    atomicMax(&S.box[k + 3], b[k + 3]);
+                }
+            }
+        }
+        __syncthreads();
+        const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
+        const bool any = lo0 <= S.box[3];
+        const int nx = any ? S.box[3] - lo0 + 1 : 0, ny = any ? S.box[4] - lo1 + 1 : 0,
+                  nz = any ? S.box[5] - lo2 + 1 : 0;
+        int ncell = 0;
+        if (any) {
+            if (nx * ny * nz > kTileCellsMax) {
+                if (tid == 0) S.defer_all = 1;
+            } else {
+                ncell = nx * ny * nz;
+            }
+        }
+        uint32_t c_cnt[kTileCellsPerThread];
+        uint32_t tsum = 0u;
+#pragma unroll
+        for (int k = 0; k < kTileCellsPerThread; ++k) {
+            const int c = kTileCellsPerThread * tid + k;
+            c_cnt[k] = 0u;
+            if (c < ncell) {
+                const int ix = c / (ny * nz), rem = c - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
+                const uint2 r = __ldg(a.cells + cell_index_of(lo0 + ix, lo1 + iy, lo2 + iz));
+                if (r.x != 0xffffffffu) {
+                    c_cnt[k] = r.y - r.x + 1u;
+                    S.first[c] = r.x;
+                }
+            }
+            tsum += c_cnt[k];
+        }
+        uint32_t inc = tsum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) S.wsum[tid >> 5] = inc;
+        __syncthreads();
+        uint32_t wbase = 0u;
+        for (int w = 0; w < (tid >> 5); ++w) wbase += S.wsum[w];
+        uint32_t run = wbase + inc - tsum;
+#pragma unroll
+        for (int k = 0; k < kTileCellsPerThread; ++k) {
+            const int c = kTileCellsPerThread * tid + k;
+            if (c < ncell) S.off[c] = run;
+            run += c_cnt[k];
+        }
+        if (tid == kTileThreads - 1) {
+            S.off[ncell] = run;
+            if (run > (uint32_t)kTileAccStage) S.defer_all = 1;
+        }
+        __syncthreads();
+        if (!S.defer_all) {
+            const uint32_t total = S.off[ncell];
+            for (uint32_t s = tid; s < total; s += kTileThreads) {
+                int lo = 0, hi = ncell - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S.off[mid] <= s) lo = mid;
+                    else hi = mid - 1;
+                }
+                const uint32_t gi = S.first[lo] + (s - S.off[lo]);
+                S.pos[s] = __ldg(a.sA + gi);
+                S.gidx[s] = gi;
+                const int ix = lo / (ny * nz), rem = lo - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
+                S.scell[s] = (uint32_t)ix | ((uint32_t)iy << 10) | ((uint32_t)iz << 20);
+            }
+        }
+        __syncthreads();
+        int wmin = 0x7fffffff;
+        for (;;) {
+            uint32_t j = 0u;
+            if (lane == 0) j = atomicAdd(&S.next, 4u);
+            j = __shfl_sync(0xffffffffu, j, 0);
+            if (start + j >= end) break;
+            wmin = min(wmin, accel_tile_warp<KAHAN>(a, S, start + j, end, lane, tid >> 5, deferred, ctr + 2));
+        }
+        if (lane == 0 && wmin != 0x7fffffff) atomicMin(&S.dtmin, wmin);
+    }
+    if (tid == 0 && S.dtmin != 0x7fffffff) atomicMin(a.globals + 1, S.dtmin);
 }
 
 struct StepArgs {
@@ -1426,6 +1836,10 @@ int tile_smem_opt_in() {
     if (dev < 0 || dev >= 64) dev = 0;
     if (!sms[dev]) {
         cudaFuncSetAttribute(k_density_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileShared));
+        cudaFuncSetAttribute(k_acceleration_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(TileAccShared));
+        cudaFuncSetAttribute(k_acceleration_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(TileAccShared));
         int v = 0;
         cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
         sms[dev] = v > 0 ? v : 148;
@@ -1512,11 +1926,34 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     a.globals = ctx->globals;
     constexpr int parts = parts_per_block<kLanesPerParticle>();
     const size_t smem = list_smem_opt_in();
+    const bool kahan = ctx->form.precision == SPH_PRECISION_MIXED;
+#ifdef SPH_PARITY
+    // one lane per particle, in the reference's order
     const unsigned blocks = (unsigned)((n + parts - 1) / parts);
-    if (ctx->form.precision == SPH_PRECISION_MIXED)
+    if (kahan)
         k_acceleration<kLanesPerParticle, true><<<blocks, parts * kLanesPerParticle, smem, st>>>(a);
     else
         k_acceleration<kLanesPerParticle, false><<<blocks, parts * kLanesPerParticle, smem, st>>>(a);
+#else
+    // the density pass's tiles, rebuilt so the pass also stands alone; its own
+    // counters (tile_ctr[4..7])
+    const int sms = tile_smem_opt_in();
+    uint32_t *ctr = ctx->tile_ctr + 4;
+    cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * 4, st);
+    k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->cell_sort.keys[ctx->cell_final], ctx->cell_range,
+                                                   ctx->tiles, ctr, nullptr);
+    if (kahan) {
+        k_acceleration_tile<true><<<sms * 2, kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
+                                                                                         ctx->deferred);
+        k_acceleration_deferred<kLanesPerParticle, true>
+            <<<sms * 8, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
+    } else {
+        k_acceleration_tile<false><<<sms * 2, kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
+                                                                                          ctx->deferred);
+        k_acceleration_deferred<kLanesPerParticle, false>
+            <<<sms * 8, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
+    }
+#endif
     return cuda_status(cudaGetLastError(), "acceleration");
 }
 

@@ -152,9 +152,10 @@ struct sph_ctx {
     int cell_final = 1;            // buffer index of the sorted cell keys
 
     float4 *sp4 = nullptr, *sv4 = nullptr, *sA = nullptr, *sB = nullptr, *sC = nullptr;
-    // density over cell tiles: (first, end) sorted range of each occupied
-    // octet; counters [0] tiles, [1] tile ticket, [2] deferred, [3] spare;
-    // the sorted indices handed to the per-particle pass
+    // density and acceleration over cell tiles: (first, end) sorted range of
+    // each tile; counters [0] tiles, [1] tile ticket, [2] deferred, [3] spare
+    // for the density pass, [4..7] the same for the acceleration pass; the
+    // sorted indices handed to the per-particle pass
     uint2 *tiles = nullptr;
     uint32_t *tile_ctr = nullptr;
     uint32_t *deferred = nullptr;
