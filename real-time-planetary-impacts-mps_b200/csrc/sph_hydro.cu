@@ -54,6 +54,16 @@ __device__ __forceinline__ float pair_rinv(float r2, float r) {
 #endif
 }
 
+// a / b in the pair arithmetic: the correctly rounded quotient in the parity
+// build, the hardware approximation (within 2 ulp) in the product.
+__device__ __forceinline__ float pdiv(float a, float b) {
+#ifdef SPH_PARITY
+    return a / b;
+#else
+    return __fdividef(a, b);
+#endif
+}
+
 // Lanes per particle in the density and acceleration walks.  The parity
 // build (SPH_PARITY) uses one, which sums in the reference's sequential order.
 #ifdef SPH_PARITY
@@ -1173,7 +1183,7 @@ __device__ __forceinline__ void accel_pair(const AccelI &I, AccelSum &S, const f
     const float r = pair_sqrt(r2);
     const float r1 = pair_rinv(r2, r);
     const float mj = Cj.x, factj = Cj.y, rhoj = Cj.z, Balj = Cj.w;
-    const float hj1 = 1.f / hj;
+    const float hj1 = pdiv(1.f, hj);
     const float vx = I.vxi - Bj.x, vy = I.vyi - Bj.y, vz = I.vzi - Bj.z;
     const float rhoij = 0.5f * (I.rhoi + rhoj);
     const float vdr = vx * dx + vy * dy + vz * dz;
@@ -1181,7 +1191,7 @@ __device__ __forceinline__ void accel_pair(const AccelI &I, AccelSum &S, const f
     const float vsig = I.ci + Bj.w - 3.f * mu;
     S.vsig = fmax_ref(vsig, S.vsig);
     const float Bij = 0.5f * (I.Bi + Balj);
-    const float nu = -0.5f * kViscosityAlpha * Bij * mu * vsig / rhoij;
+    const float nu = pdiv(-0.5f * kViscosityAlpha * Bij * mu * vsig, rhoij);
     const float rhx = dx * r1, rhy = dy * r1, rhz = dz * r1;
     const float si = kernel_gradw_scale(r, I.hi1), sj = kernel_gradw_scale(r, hj1);
     const float gix = si * rhx, giy = si * rhy, giz = si * rhz;
@@ -1192,7 +1202,7 @@ __device__ __forceinline__ void accel_pair(const AccelI &I, AccelSum &S, const f
     accel_add<KAHAN>(S.dvz, S.kz, -(mj * (I.facti * giz + factj * gjz + nu * gz)));
     accel_add<KAHAN>(S.du, S.ku,
                      mj * (I.facti * (vx * gix + vy * giy + vz * giz) + 0.5f * nu * (vx * gx + vy * gy + vz * gz)));
-    accel_add<KAHAN>(S.dh, S.kh, (mj / rhoj) * (vx * gix + vy * giy + vz * giz));
+    accel_add<KAHAN>(S.dh, S.kh, pdiv(mj, rhoj) * (vx * gix + vy * giy + vz * giz));
 }
 // The group's sums combined (every lane ends with the same bits).
 template <int L, bool KAHAN>
@@ -1353,6 +1363,7 @@ struct TileAccShared {
     uint32_t start, end, tile, next;
     int defer_all;
     int dtmin;
+    int hmax_bits;                      // largest staged h (float bits; h > 0)
 };
 
 // The reference's box of an acceleration particle and whether the tile path
@@ -1421,13 +1432,16 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
               v2 = __reduce_max_sync(kFull, b.hi2);
     if (u0 > v0) return 0x7fffffff;  // no active particle takes the tile path
     __syncwarp();
-    float qx[4], qy[4], qz[4], qr[4];
+    // every accepted pair lies within 2 max(h_i, largest staged h) of the particle
+    const float hm = fmaxf(I.hi, __int_as_float(S.hmax_bits));
+    float qx[4], qy[4], qz[4], qr[4], qR[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         qx[k] = __shfl_sync(kFull, I.xi, k * L);
         qy[k] = __shfl_sync(kFull, I.yi, k * L);
         qz[k] = __shfl_sync(kFull, I.zi, k * L);
         qr[k] = __shfl_sync(kFull, want ? I.hi2x4 : -1.f, k * L);
+        qR[k] = __shfl_sync(kFull, want ? 4.f * hm * hm : -1.f, k * L);
     }
     // box bounds of the four groups, for the row test (lane k * L holds group k's)
     int cnt[4] = {0, 0, 0, 0};
@@ -1443,15 +1457,24 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
             x = u0 + r / nyu;
             y = u1 + r % nyu;
         }
-        // the z range of the boxes that contain row (x, y)
+        // the z range of the boxes that contain row (x, y), trimmed to the
+        // sphere that holds every accepted pair
+        constexpr float w = kCellWidth;
+        constexpr float iw = 1.f / kCellWidth;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int bl0 = __shfl_sync(kFull, b.lo0, k * L), bh0 = __shfl_sync(kFull, b.hi0, k * L);
             const int bl1 = __shfl_sync(kFull, b.lo1, k * L), bh1 = __shfl_sync(kFull, b.hi1, k * L);
             const int bl2 = __shfl_sync(kFull, b.lo2, k * L), bh2 = __shfl_sync(kFull, b.hi2, k * L);
             if (r < rows && x >= bl0 && x <= bh0 && y >= bl1 && y <= bh1) {
-                zl = min(zl, bl2);
-                zh = max(zh, bh2);
+                const float gx = fmaxf(fmaxf((float)x * w - qx[k], qx[k] - (float)(x + 1) * w) - kCellMargin, 0.f);
+                const float gy = fmaxf(fmaxf((float)y * w - qy[k], qy[k] - (float)(y + 1) * w) - kCellMargin, 0.f);
+                const float g2 = gx * gx + gy * gy;
+                if (g2 <= qR[k]) {
+                    const float dz = sqrtf(qR[k] - g2);
+                    zl = min(zl, max(bl2, (int)floorf((qz[k] - dz) * iw - 1e-3f)));
+                    zh = max(zh, min(bh2, (int)floorf((qz[k] + dz) * iw + 1e-3f)));
+                }
             }
         }
         if (zl <= zh) {
@@ -1555,6 +1578,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             S.box[0] = S.box[1] = S.box[2] = 0x7fffffff;
             S.box[3] = S.box[4] = S.box[5] = -0x7fffffff;
             S.defer_all = 0;
+            S.hmax_bits = 0;
         }
         __syncthreads();
         if (S.tile >= ntiles) break;
@@ -1637,6 +1661,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             if (run > (uint32_t)kTileAccStage) S.defer_all = 1;
         }
         __syncthreads();
+        float hmax = 0.f;
         if (!S.defer_all) {
             const uint32_t total = S.off[ncell];
             for (uint32_t s = tid; s < total; s += kTileThreads) {
@@ -1647,11 +1672,19 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                     else hi = mid - 1;
                 }
                 const uint32_t gi = S.first[lo] + (s - S.off[lo]);
-                S.pos[s] = __ldg(a.sA + gi);
+                const float4 q = __ldg(a.sA + gi);
+                S.pos[s] = q;
                 S.gidx[s] = gi;
                 const int ix = lo / (ny * nz), rem = lo - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
                 S.scell[s] = (uint32_t)ix | ((uint32_t)iy << 10) | ((uint32_t)iz << 20);
+                hmax = fmaxf(hmax, q.w);
             }
+        }
+        {
+            float v = hmax;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if (lane == 0 && v > 0.f) atomicMax(&S.hmax_bits, __float_as_int(v));
         }
         __syncthreads();
         int wmin = 0x7fffffff;
