@@ -316,6 +316,41 @@ sph_status sph_clear_health(sph_ctx *ctx);
  * FP32 FMA peak of the device. */
 sph_status sph_probe_fp32_fma(int32_t blocks, int32_t iters, float *sink, void *stream);
 
+/* Batched ensemble (no counterpart in the reference, which runs one impact per
+ * process: Headless.cpp:43-51).  n_instances independent impacts on the
+ * current device, each with its own initial conditions and form (forms may be
+ * NULL: all defaults) and the shared params; each instance is a full context
+ * (reachable through sph_ensemble_instance for uploads, downloads and
+ * diagnostics).  sph_ensemble_step advances every instance by n_steps steps,
+ * one launch of one CUDA graph per step whose branches are the instances'
+ * full steps, so small instances run side by side on the device.
+ * With autotune != 0 the tuner picks per instance, on a scratch copy made from
+ * the same initial conditions (the instance itself is not advanced): the
+ * density / acceleration tile size, by timing, and for SPH_GRAVITY_THETA the
+ * leaf capacity among 1, 2 and 4 times params->max_children_in_leaf, by timing
+ * among those whose gravity has a median relative error <= 1e-3 against the
+ * FP64 direct sum on 512 targets.  sph_ensemble_get_tuning reports the choice.
+ * Creation synchronises the device.  Stepping is asynchronous on `stream`;
+ * the first sph_ensemble_step call runs its first step eagerly, waits for it
+ * and captures the step graph (so make it outside any stream capture), as
+ * sph_step_all does.  sph_ensemble_synchronize waits and checks every
+ * instance's health word. */
+typedef struct sph_ensemble sph_ensemble;
+typedef struct {
+    int32_t max_children_in_leaf; /* leaf capacity the instance runs with */
+    uint32_t tile_block_max;      /* particles of a 64-cell density / acceleration tile before it is split */
+    float ms_per_step;            /* the tuner's time of one full step with this choice (0: not tuned) */
+    float gravity_median_error;   /* its gravity error on the tuning sample (-1: not checked) */
+} sph_ensemble_tuning;
+sph_status sph_ensemble_create(const sph_params *params, int32_t n_instances, const sph_ic *ics,
+                               const sph_form *forms, int32_t autotune, sph_ensemble **out);
+sph_status sph_ensemble_destroy(sph_ensemble *e);
+int32_t sph_ensemble_size(const sph_ensemble *e);
+sph_status sph_ensemble_instance(sph_ensemble *e, int32_t i, sph_ctx **ctx);
+sph_status sph_ensemble_get_tuning(const sph_ensemble *e, int32_t i, sph_ensemble_tuning *out);
+sph_status sph_ensemble_step(sph_ensemble *e, void *stream, int32_t n_steps);
+sph_status sph_ensemble_synchronize(sph_ensemble *e, void *stream);
+
 /* Host-only helpers (no GPU work). */
 /* ANEOS.cpp:21-175: parse a table and resample it to res x res (pressure,
  * sound speed) pairs, rho rows, u columns.  out holds 2*res*res floats. */

@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(HERE, "libsph_b200.so")
 PARITY_LIB_PATH = os.path.join(HERE, "libsph_b200_parity.so")
 PARITY_FLAGS = ["-fmad=false", "-DSPH_PARITY"]
 SOURCES = ["sph_api.cu", "sph_sort.cu", "sph_hydro.cu", "sph_gravity.cu", "sph_gravity_theta.cu", "sph_tree.cu",
-           "sph_hseed.cu"]
+           "sph_hseed.cu", "sph_ensemble.cu"]
 HEADERS = ["sph_common.cuh", "sph_internal.h", "sph_tc.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared"]
@@ -73,6 +73,11 @@ class SphIC(C.Structure):
 class SphForm(C.Structure):
     _fields_ = [("gravity", C.c_int32), ("theta", C.c_float), ("h_seed", C.c_int32), ("precision", C.c_int32),
                 ("h_tolerance", C.c_float)]
+
+
+class SphEnsembleTuning(C.Structure):
+    _fields_ = [("max_children_in_leaf", C.c_int32), ("tile_block_max", C.c_uint32), ("ms_per_step", C.c_float),
+                ("gravity_median_error", C.c_float)]
 
 
 class SphHSeedStats(C.Structure):
@@ -199,6 +204,14 @@ def load(parity: bool = False) -> C.CDLL:
         "sph_get_health": (st, [vp, C.POINTER(C.c_uint32)]),
         "sph_clear_health": (st, [vp]),
         "sph_eos_resample": (st, [C.c_char_p, C.c_int32, _fp]),
+        "sph_ensemble_create": (st, [C.POINTER(SphParams), C.c_int32, C.POINTER(SphIC), C.POINTER(SphForm), C.c_int32,
+                                     C.POINTER(vp)]),
+        "sph_ensemble_destroy": (st, [vp]),
+        "sph_ensemble_size": (C.c_int32, [vp]),
+        "sph_ensemble_instance": (st, [vp, C.c_int32, C.POINTER(vp)]),
+        "sph_ensemble_get_tuning": (st, [vp, C.c_int32, C.POINTER(SphEnsembleTuning)]),
+        "sph_ensemble_step": (st, [vp, vp, C.c_int32]),
+        "sph_ensemble_synchronize": (st, [vp, vp]),
         "sph_status_string": (C.c_char_p, [st]),
         "sph_last_error": (C.c_char_p, []),
     }

@@ -41,6 +41,57 @@ def _ptr(a: np.ndarray, t):
     return a.ctypes.data_as(t)
 
 
+def _tables(forsterite_table, fe85si15_table):
+    if forsterite_table is None or fe85si15_table is None:
+        tabs = eos_tables.ensure_tables()
+        forsterite_table = forsterite_table or tabs["forsterite"]
+        fe85si15_table = fe85si15_table or tabs["Fe85Si15"]
+    if not os.path.exists(forsterite_table) or not os.path.exists(fe85si15_table):
+        raise FileNotFoundError("ANEOS tables not found")
+    return forsterite_table.encode(), fe85si15_table.encode()
+
+
+def _params(lib, paths, max_children_in_leaf, max_tree_depth, max_unchecked_pointers, aneos_resolution,
+            tree_source) -> "_lib.SphParams":
+    p = _lib.SphParams()
+    lib.sph_params_default(C.byref(p))
+    p.max_children_in_leaf = max_children_in_leaf
+    p.max_tree_depth = max_tree_depth
+    p.max_unchecked_pointers = max_unchecked_pointers
+    p.aneos_resolution = aneos_resolution
+    p.tree_source = _lib.SPH_TREE_GPU if tree_source == "gpu" else _lib.SPH_TREE_HOST
+    p.forsterite_table = paths[0]
+    p.fe85si15_table = paths[1]
+    return p
+
+
+def _ic_struct(ic: dict):
+    """(SphIC, the arrays it points into -- keep them alive while it is used)."""
+    n = int(np.asarray(ic["pos"]).reshape(-1, 3).shape[0])
+    f32 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float32).reshape(-1))  # noqa: E731
+    keep = dict(pos=f32(ic["pos"]), vel=f32(ic["vel"]), rho=f32(ic["rho"]), u=f32(ic["u"]),
+                mass=f32(ic["mass"]), pressure=f32(ic.get("pressure", np.zeros(n))), h=f32(ic["h"]),
+                material=np.ascontiguousarray(np.asarray(ic["material"], dtype=np.int32).reshape(-1)))
+    s = _lib.SphIC()
+    s.n = n
+    for k in ("pos", "vel", "rho", "u", "mass", "pressure", "h"):
+        setattr(s, k, _ptr(keep[k], _fp))
+    s.material = _ptr(keep["material"], _ip)
+    return s, keep
+
+
+def _form(lib, gravity: str = "reference", theta: float = 0.5, precision: str = "reference",
+          h_seed: str = "plain", h_tolerance: float = 0.0) -> "_lib.SphForm":
+    f = _lib.SphForm()
+    lib.sph_form_default(C.byref(f))
+    f.gravity = _lib.SPH_GRAVITY_THETA if gravity == "theta" else _lib.SPH_GRAVITY_REFERENCE
+    f.theta = float(theta)
+    f.precision = _lib.SPH_PRECISION_MIXED if precision == "mixed" else _lib.SPH_PRECISION_REFERENCE
+    f.h_seed = _lib.SPH_HSEED_LEARNED if h_seed == "learned" else _lib.SPH_HSEED_PLAIN
+    f.h_tolerance = float(h_tolerance)
+    return f
+
+
 class Compute:
     """One simulation on the current CUDA device."""
 
@@ -52,38 +103,30 @@ class Compute:
         # reference's sequential order); only tests use it
         lib = _lib.load(parity)
         self._lib = lib
-        if forsterite_table is None or fe85si15_table is None:
-            tabs = eos_tables.ensure_tables()
-            forsterite_table = forsterite_table or tabs["forsterite"]
-            fe85si15_table = fe85si15_table or tabs["Fe85Si15"]
-        if not os.path.exists(forsterite_table) or not os.path.exists(fe85si15_table):
-            raise FileNotFoundError("ANEOS tables not found")
-        p = _lib.SphParams()
-        lib.sph_params_default(C.byref(p))
-        p.max_children_in_leaf = max_children_in_leaf
-        p.max_tree_depth = max_tree_depth
-        p.max_unchecked_pointers = max_unchecked_pointers
-        p.aneos_resolution = aneos_resolution
-        p.tree_source = _lib.SPH_TREE_GPU if tree_source == "gpu" else _lib.SPH_TREE_HOST
-        self._paths = (forsterite_table.encode(), fe85si15_table.encode())
-        p.forsterite_table = self._paths[0]
-        p.fe85si15_table = self._paths[1]
-        n = int(np.asarray(ic["pos"]).reshape(-1, 3).shape[0])
-        f32 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float32).reshape(-1))  # noqa: E731
-        keep = dict(pos=f32(ic["pos"]), vel=f32(ic["vel"]), rho=f32(ic["rho"]), u=f32(ic["u"]),
-                    mass=f32(ic["mass"]), pressure=f32(ic.get("pressure", np.zeros(n))), h=f32(ic["h"]),
-                    material=np.ascontiguousarray(np.asarray(ic["material"], dtype=np.int32).reshape(-1)))
-        s = _lib.SphIC()
-        s.n = n
-        for k in ("pos", "vel", "rho", "u", "mass", "pressure", "h"):
-            setattr(s, k, _ptr(keep[k], _fp))
-        s.material = _ptr(keep["material"], _ip)
+        self._paths = _tables(forsterite_table, fe85si15_table)
+        p = _params(lib, self._paths, max_children_in_leaf, max_tree_depth, max_unchecked_pointers,
+                    aneos_resolution, tree_source)
+        s, keep = _ic_struct(ic)
+        n = s.n
         h = C.c_void_p()
         _lib.check(lib.sph_create(C.byref(p), C.byref(s), C.byref(h)), "sph_create", lib)
         self._lib = lib
         self._h = h
+        self._owned = True
         self.nParticles = n
         self.tree_source = tree_source
+
+    @classmethod
+    def _borrow(cls, lib, handle: C.c_void_p, tree_source: str = "gpu") -> "Compute":
+        """A Compute over a context another object owns (an ensemble
+        instance); closing it does not destroy the context."""
+        c = cls.__new__(cls)
+        c._lib = lib
+        c._h = handle
+        c._owned = False
+        c.nParticles = int(lib.sph_num_particles(handle))
+        c.tree_source = tree_source
+        return c
 
     def _check(self, status: int, what: str):
         _lib.check(status, what, self._lib)
@@ -91,7 +134,8 @@ class Compute:
     # ---- lifetime ------------------------------------------------------
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
-            self._lib.sph_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self._lib.sph_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
@@ -184,13 +228,7 @@ class Compute:
         positions and time, Kahan-compensated sums); h_seed "plain" or
         "learned" (the trained MLP starts the density iteration);
         h_tolerance of the density iteration (0 = the reference's 0.005)."""
-        f = _lib.SphForm()
-        self._lib.sph_form_default(C.byref(f))
-        f.gravity = _lib.SPH_GRAVITY_THETA if gravity == "theta" else _lib.SPH_GRAVITY_REFERENCE
-        f.theta = float(theta)
-        f.precision = _lib.SPH_PRECISION_MIXED if precision == "mixed" else _lib.SPH_PRECISION_REFERENCE
-        f.h_seed = _lib.SPH_HSEED_LEARNED if h_seed == "learned" else _lib.SPH_HSEED_PLAIN
-        f.h_tolerance = float(h_tolerance)
+        f = _form(self._lib, gravity, theta, precision, h_seed, h_tolerance)
         self._check(self._lib.sph_set_form(self._h, C.byref(f)), "sph_set_form")
 
     def get_form(self) -> dict:
@@ -356,6 +394,86 @@ class Compute:
         names = ("pos", "vel", "acc", "rho", "u", "mass", "pressure", "h", "grad_term", "sound_speed", "du",
                  "balsara", "dhdt", "grav_norm", "material", "active", "next_active_time", "global_time", "dt")
         return {k: self.download(k) for k in names}
+
+
+class Ensemble:
+    """Many independent impacts advanced together on the current device
+    (sph_ensemble_*; no counterpart in the reference).  `forms` holds one
+    set_form keyword dict per instance (or None: the defaults); autotune picks
+    each instance's tile size and, for the theta form, its leaf capacity.
+    `instances` are Compute views of the instances' contexts."""
+
+    def __init__(self, ics: list, forms: list | None = None, *, autotune: bool = False,
+                 max_children_in_leaf: int = 32, max_tree_depth: int = 7, max_unchecked_pointers: int = 1024,
+                 aneos_resolution: int = 2048, tree_source: str = "gpu", forsterite_table: str | None = None,
+                 fe85si15_table: str | None = None):
+        lib = _lib.load()
+        self._lib = lib
+        self._paths = _tables(forsterite_table, fe85si15_table)
+        p = _params(lib, self._paths, max_children_in_leaf, max_tree_depth, max_unchecked_pointers,
+                    aneos_resolution, tree_source)
+        k = len(ics)
+        structs = (_lib.SphIC * k)()
+        keep = []
+        for i, ic in enumerate(ics):
+            s, arrays = _ic_struct(ic)
+            structs[i] = s
+            keep.append(arrays)
+        fa = None
+        if forms is not None:
+            fa = (_lib.SphForm * k)()
+            for i, f in enumerate(forms):
+                fa[i] = _form(lib, **(f or {}))
+        h = C.c_void_p()
+        _lib.check(lib.sph_ensemble_create(C.byref(p), k, structs, fa, 1 if autotune else 0, C.byref(h)),
+                   "sph_ensemble_create", lib)
+        self._h = h
+        self.instances = []
+        for i in range(k):
+            c = C.c_void_p()
+            _lib.check(lib.sph_ensemble_instance(h, i, C.byref(c)), "sph_ensemble_instance", lib)
+            self.instances.append(Compute._borrow(lib, c, tree_source))
+        self.sizes = [c.nParticles for c in self.instances]
+
+    def __len__(self):
+        return len(self.instances)
+
+    def step(self, n_steps: int = 1, stream=None):
+        _lib.check(self._lib.sph_ensemble_step(self._h, _stream(stream), int(n_steps)), "sph_ensemble_step",
+                   self._lib)
+
+    def synchronize(self, stream=None):
+        _lib.check(self._lib.sph_ensemble_synchronize(self._h, _stream(stream)), "sph_ensemble_synchronize",
+                   self._lib)
+
+    def tuning(self) -> list:
+        out = []
+        for i in range(len(self.instances)):
+            t = _lib.SphEnsembleTuning()
+            _lib.check(self._lib.sph_ensemble_get_tuning(self._h, i, C.byref(t)), "sph_ensemble_get_tuning",
+                       self._lib)
+            out.append(dict(max_children_in_leaf=t.max_children_in_leaf, tile_block_max=t.tile_block_max,
+                            ms_per_step=t.ms_per_step, gravity_median_error=t.gravity_median_error))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            for c in self.instances:
+                c.close()
+            self._lib.sph_ensemble_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def eos_resample(path: str, res: int = 2048) -> np.ndarray:

@@ -1013,7 +1013,12 @@ sph_status sph_step(sph_ctx *ctx, void *stream) {
     return ctx ? launch_step(ctx, (cudaStream_t)stream) : SPH_ERR_INVALID_ARG;
 }
 
-static sph_status one_step(sph_ctx *ctx, cudaStream_t st) {
+}  // extern "C"
+
+namespace sph {
+
+// One full step (Headless.cpp:43-51 without the snapshot) on `st`.
+sph_status full_step(sph_ctx *ctx, cudaStream_t st) {
     sph_status s = SPH_OK;
     if (ctx->params.tree_source == SPH_TREE_GPU) s = launch_tree_build(ctx, st);
     if (s == SPH_OK) s = launch_sort(ctx, st);
@@ -1023,6 +1028,10 @@ static sph_status one_step(sph_ctx *ctx, cudaStream_t st) {
     if (s == SPH_OK) s = launch_step(ctx, st);
     return s;
 }
+
+}  // namespace sph
+
+extern "C" {
 
 sph_status sph_step_all(sph_ctx *ctx, void *stream, int32_t n_steps) {
     if (!ctx || n_steps < 0) return SPH_ERR_INVALID_ARG;
@@ -1035,7 +1044,7 @@ sph_status sph_step_all(sph_ctx *ctx, void *stream, int32_t n_steps) {
     if (!ctx->graph) {
         // capture one full step on a private stream; the buffer roles of the
         // sort (cell_final, cells_have_prev) are the same every step once warm
-        sph_status s = one_step(ctx, st);  // warm: establishes the steady buffer roles
+        sph_status s = full_step(ctx, st);  // warm: establishes the steady buffer roles
         if (s != SPH_OK) return s;
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return cuda_status(e, "sph_step_all warm step");
@@ -1043,7 +1052,7 @@ sph_status sph_step_all(sph_ctx *ctx, void *stream, int32_t n_steps) {
         cudaGraph_t g = nullptr;
         e = cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return cuda_status(e, "begin capture");
-        s = one_step(ctx, ctx->own_stream);
+        s = full_step(ctx, ctx->own_stream);
         e = cudaStreamEndCapture(ctx->own_stream, &g);
         if (s != SPH_OK) {
             if (g) cudaGraphDestroy(g);

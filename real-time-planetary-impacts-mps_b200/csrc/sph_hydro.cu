@@ -569,8 +569,6 @@ constexpr int kTileCellsMax = 1024;                         // cells of a tile's
 constexpr int kTileCellsPerThread = (kTileCellsMax + kTileThreads - 1) / kTileThreads;
 constexpr int kTileReach = 3;                               // cells a list box may extend past its own cell
 constexpr int kTileList = 256;                              // list entries per particle (staged slots)
-constexpr uint32_t kTileBlockMax = 320;                     // particles of a 64-cell tile
-constexpr uint32_t kTileHalfMax = 256;                      // particles of a 16-cell tile
 
 struct TileShared {
     float4 pos[kTileStageMax];          // staged (x, y, z, m)
@@ -621,12 +619,13 @@ __device__ __forceinline__ float tile_start_h(const DensityArgs &a, uint32_t ind
 
 // Tiles: at the first sorted particle of every occupied 64-cell block, the
 // block's octet ranges (from its 64 cell ranges); the block is one tile when it
-// holds at most kTileBlockMax particles, else each 16-cell quarter is one when
-// it holds at most kTileHalfMax, else each octet is.  (first, one past last)
+// holds at most block_max particles, else each 16-cell quarter is one when it
+// holds at most half_max, else each octet is.  (first, one past last)
 // per tile, in ticket order.  ctr[0] counts tiles; ctr[1] is the CTAs' tile
 // ticket, ctr[2] the deferred count.
 __global__ void k_tile_starts(int n, const uint32_t *__restrict__ skey, const uint2 *__restrict__ cells,
-                              uint2 *__restrict__ tiles, uint32_t *ctr, int32_t *globals) {
+                              uint2 *__restrict__ tiles, uint32_t *ctr, int32_t *globals, uint32_t block_max,
+                              uint32_t half_max) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k == 0 && globals) globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
     if (k >= n) return;
@@ -660,14 +659,14 @@ __global__ void k_tile_starts(int n, const uint32_t *__restrict__ skey, const ui
     };
     uint32_t f, l;
     span(0, 8, f, l);
-    if (l - f <= kTileBlockMax) {
+    if (l - f <= block_max) {
         emit(f, l);
         return;
     }
     for (int q = 0; q < 4; ++q) {
         span(2 * q, 2 * q + 2, f, l);
         if (l <= f) continue;
-        if (l - f <= kTileHalfMax) {
+        if (l - f <= half_max) {
             emit(f, l);
         } else {
             emit(ofirst[2 * q], oend[2 * q]);
@@ -1931,7 +1930,8 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     const int sms = tile_smem_opt_in();
     cudaMemsetAsync(ctx->tile_ctr, 0, sizeof(uint32_t) * 4, st);
     k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->cell_sort.keys[ctx->cell_final], ctx->cell_range,
-                                                   ctx->tiles, ctx->tile_ctr, ctx->globals);
+                                                   ctx->tiles, ctx->tile_ctr, ctx->globals, ctx->tile_block_max,
+                                                   ctx->tile_half_max);
     k_density_tile<<<sms * 2, kTileThreads, sizeof(TileShared), st>>>(a, ctx->tiles, ctx->tile_ctr, ctx->deferred);
     k_density_deferred<kLanesPerParticle><<<sms * 8, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred,
                                                                                            ctx->tile_ctr + 2);
@@ -1974,7 +1974,7 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     uint32_t *ctr = ctx->tile_ctr + 4;
     cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * 4, st);
     k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->cell_sort.keys[ctx->cell_final], ctx->cell_range,
-                                                   ctx->tiles, ctr, nullptr);
+                                                   ctx->tiles, ctr, nullptr, ctx->tile_block_max, ctx->tile_half_max);
     if (kahan) {
         k_acceleration_tile<true><<<sms * 2, kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
                                                                                          ctx->deferred);

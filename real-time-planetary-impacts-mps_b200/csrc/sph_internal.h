@@ -159,6 +159,10 @@ struct sph_ctx {
     uint2 *tiles = nullptr;
     uint32_t *tile_ctr = nullptr;
     uint32_t *deferred = nullptr;
+    // tile sizes: a 64-cell block is one tile up to tile_block_max particles,
+    // else its 16-cell quarters up to tile_half_max, else its octets
+    uint32_t tile_block_max = 320;
+    uint32_t tile_half_max = 256;
     float2 *eos_forsterite = nullptr, *eos_fe = nullptr;
     sph::EosTables eos{};
 
@@ -230,6 +234,8 @@ void tree_free(sph_ctx *ctx);
 sph_status launch_tree_build(sph_ctx *ctx, cudaStream_t st);
 
 // sph_api.cu
+// One full step (tree, sort, gravity, density, acceleration, step) on st.
+sph_status full_step(sph_ctx *ctx, cudaStream_t st);
 void set_error(const char *fmt, ...);
 sph_status cuda_status(cudaError_t e, const char *what);
 
