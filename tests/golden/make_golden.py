@@ -28,6 +28,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle as O  # noqa: E402
 
 pkg_ic = importlib.import_module("real-time-planetary-impacts-mps_b200.ic")
+pkg_h5 = importlib.import_module("real-time-planetary-impacts-mps_b200.hdf5io")
 pkg_eos = importlib.import_module("real-time-planetary-impacts-mps_b200.eos_tables")
 
 PASS_OUTPUTS = {
@@ -104,6 +105,30 @@ def main(ref_root: str | None = None):
                 names.append(f"s{s}_{p}_{f}")
     np.savez_compressed(os.path.join(HERE, "config0_digests.npz"), names=np.array(names), digests=np.stack(digests),
                         final_pos=st.pos, final_vel=st.vel, final_u=st.u, final_h=st.h, final_rho=st.rho)
+    # 6. the reference's own input file, SPH/demo_impact_n40.hdf5, read as
+    # readHDFFile does (hdfHandler.cpp:12-136); two full steps at the
+    # reference's default leaf capacity (4) on its CPU octree.  Kept: the
+    # initial conditions, both steps' trees, every pass output of step 0 and
+    # the step-pass outputs of step 1.
+    demo = os.path.join(ref_root, "SPH", "demo_impact_n40.hdf5")
+    ic = pkg_h5.read_ic(demo)
+    with open(demo, "rb") as f:
+        file_digest = np.frombuffer(hashlib.sha256(f.read()).digest(), np.uint8)
+    st = O.OracleState(ic, ef, ee, kind="ref")
+    out = {f"ic_{k}": np.asarray(v) for k, v in ic.items() if isinstance(v, np.ndarray)}
+    out["file_sha256"] = file_digest
+    for s in range(2):
+        t = O.tree_reference(st.pos, 4, kind="ref")
+        st.set_tree(t)
+        for k in ("tree", "level_offsets", "level_nodes"):
+            out[f"s{s}_tree_{k}"] = t[k]
+        out[f"s{s}_tree_meta"] = np.array([t["n_levels"], t["n_nodes"]], np.int32)
+        for p, fields in PASS_OUTPUTS.items():
+            getattr(st, p)()
+            if s == 0 or p == "step":
+                for f in fields:
+                    out[f"s{s}_{p}_{f}"] = getattr(st, f).copy()
+    np.savez_compressed(os.path.join(HERE, "demo_impact_n40.npz"), **out)
     print("fixtures written to", HERE)
 
 

@@ -58,3 +58,35 @@ def test_fma_contraction_moves_reference_gravity_by_about_1e3(O, eos_grids, tmp_
     for f in ("h", "rho"):
         x, y = getattr(a, f).astype(np.float64), getattr(b, f).astype(np.float64)
         assert np.max(np.abs(x - y) / np.abs(x)) < 1e-6, f
+
+
+@pytest.mark.skipif(not _has_fma(), reason="host CPU without FMA")
+def test_fma_contraction_on_the_reference_demo_file(O, eos_grids, tmp_path):
+    """The same yardstick on the reference's own input (demo_impact_n40): its
+    leaf-4 tree and larger smoothing lengths make gravity more sensitive, max
+    ~5.7e-3, p99 ~1.4e-4 -- the basis of that input's product tolerance."""
+    src = os.path.join(os.path.dirname(O.__file__), "oracle.cpp")
+    so = str(tmp_path / "liboracle_fma.so")
+    subprocess.run(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-mfma", "-ffp-contract=fast",
+                    "-o", so, src], check=True)
+    lib = C.CDLL(so)
+    O._bind(lib, "ora")
+    g = golden("demo_impact_n40.npz")
+    ic = {k[3:]: v for k, v in g.items() if k.startswith("ic_")}
+    tree = dict(tree=g["s0_tree_tree"], level_offsets=g["s0_tree_level_offsets"],
+                level_nodes=g["s0_tree_level_nodes"], n_levels=int(g["s0_tree_meta"][0]),
+                n_nodes=int(g["s0_tree_meta"][1]))
+    a = O.OracleState(ic, *eos_grids)
+    b = O.OracleState(ic, *eos_grids)
+    b.lib = lib
+    for s in (a, b):
+        s.set_tree(tree)
+        s.sort()
+        s.gravity()
+    assert np.array_equal(a.acc, g["s0_gravity_acc"])  # the plain build is the reference's gravity
+    x, y = a.acc.astype(np.float64), b.acc.astype(np.float64)
+    scale = np.sqrt(np.mean((x * x).sum(1)))
+    e = np.linalg.norm(x - y, axis=1) / np.maximum(np.linalg.norm(x, axis=1), 1e-3 * scale)
+    assert 1e-3 < e.max() < 6e-3
+    assert np.percentile(e, 99) < 1e-3
+

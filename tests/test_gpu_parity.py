@@ -159,6 +159,48 @@ def test_every_pass_matches_reference_two_steps(cuda, pkg, build):
                     compare(f, c.download(f), g[f"s{s}_{p}_{f}"], f"{build} step {s} {p}", tol, p99)
 
 
+@pytest.mark.parametrize("build", ["product", "parity"])
+def test_demo_file_steps_match_reference(cuda, pkg, build):
+    """The reference's own input (SPH/demo_impact_n40.hdf5, 10 766 particles,
+    read by hdf5io as readHDFFile does): every pass of step 0 and the state
+    after step 1 against the reference's kernels on the same input and the
+    same CPU octree (leaf capacity 4, the reference's default); step 1 restarts
+    from the reference's state after step 0."""
+    g = golden("demo_impact_n40.npz")
+    ic = {k[3:]: v for k, v in g.items() if k.startswith("ic_")}
+    parity = build == "parity"
+    if parity:
+        pkg.build(parity=True)
+    # On this input FMA contraction alone moves the reference's own gravity by
+    # max 5.7e-3 (p99 1.4e-4; tests/test_fp_sensitivity.py); the product
+    # build's gravity-derived fields get twice that, the p99 bounds unchanged.
+    # In the parity build gravity is bit-identical; the acceleration pass's acc
+    # carries one ulp of logf/powf in the EOS table coordinate (5.9e-5 here,
+    # inside its 1e-4 bound), and v += dt a carries that into the velocity
+    # (1.3e-5 after two steps): 5e-5 for this input.
+    tol = dict(TOL_PARITY, vel=5e-5) if parity else dict(TOL_PRODUCT, acc=1.2e-2, grav_norm=1.2e-2, vel=1.2e-2)
+    p99 = P99_TOL_PARITY if parity else P99_TOL
+    print()
+    with pkg.Compute(ic, tree_source="host", max_children_in_leaf=4, parity=parity) as c:
+        for s in range(2):
+            if s == 1:
+                for f in ("pos", "vel", "u", "h", "rho"):
+                    c.upload(f, g[f"s0_step_{f}"])
+                c.upload("global_time", g["s0_step_global_time"])
+                c.upload("next_active_time", g["s0_acceleration_next_active_time"])
+                c.upload("grav_norm", g["s0_gravity_grav_norm"])
+                c.upload("active", g["s0_gravity_active"])
+                for f in ("pressure", "grad_term", "balsara", "sound_speed"):
+                    c.upload(f, g[f"s0_density_{f}"])
+            c.set_tree(tree_of(g, s))
+            for p, fields in PASS_OUTPUTS.items():
+                getattr(c, PASS_METHOD[p])()
+                c.synchronize()
+                if s == 0 or p == "step":
+                    for f in fields:
+                        compare(f, c.download(f), g[f"s{s}_{p}_{f}"], f"demo {build} step {s} {p}", tol, p99)
+
+
 def test_gpu_tree_matches_oracle_morton_tree(cuda, pkg, O):
     ic = pkg.ic.make_impact(16384, 4096, seed=0)
     for leaf, depth in ((4, 7), (32, 7), (32, 10)):
