@@ -97,7 +97,8 @@ typedef enum {
     SPH_FIELD_MATERIAL = 14,    /* I   materialIdBuffer */
     SPH_FIELD_ACTIVE = 15,      /* B   _active */
     SPH_FIELD_NEXT_ACTIVE = 16, /* I   _nextActiveTime */
-    SPH_FIELD_GLOBAL_TIME = 17, /* I   _globalTime (1 value, ticks of 32/65536 s) */
+    SPH_FIELD_GLOBAL_TIME = 17, /* I   _globalTime (1 value, ticks of 32/65536 s); an upload in the mixed form
+                                       also sets the FP64 time to ticks x 2^-11 s */
     SPH_FIELD_DT = 18,          /* I   _dt (1 value, ticks) */
     SPH_FIELD_CELL_KEY = 19,    /* U   _cellArrayi[].x after sort (n) */
     SPH_FIELD_CELL_INDEX = 20,  /* U   _cellArrayi[].y after sort (n) */
@@ -106,7 +107,9 @@ typedef enum {
     SPH_FIELD_POTENTIAL = 23,   /* F   gravitational potential G phi (SPH_GRAVITY_THETA only; no reference buffer) */
     SPH_FIELD_POS64 = 24,       /* D3  FP64 master positions (3n doubles) of SPH_PRECISION_MIXED; an upload also
                                        sets the float positions to their roundings */
-    SPH_FIELD_COUNT = 25
+    SPH_FIELD_NEIGHBOURS = 25,  /* F   neighbour count of the last density pass, a feature of the learned h
+                                       seed (present once the seed is in use or recording; no reference buffer) */
+    SPH_FIELD_COUNT = 26
 } sph_field;
 
 /* Defaults equal to SPH/Parameters.h (table paths are the reference's names). */
@@ -220,6 +223,11 @@ sph_status sph_hseed_train(sph_ctx *ctx, int32_t iterations, int32_t batch, floa
 sph_status sph_hseed_gradient(sph_ctx *ctx, int32_t batch, uint32_t salt, float *grads, float *loss, void *stream);
 sph_status sph_hseed_params(sph_ctx *ctx, float *get, const float *set);
 sph_status sph_hseed_dataset(sph_ctx *ctx, float *features, float *targets, float *norm);
+/* The seed network's input/target standardisation (18 floats, the layout of
+ * sph_hseed_dataset's norm): get it (after training), and/or set it, which
+ * with sph_hseed_params restores a trained network, e.g. on resume from a
+ * checkpoint.  Either pointer may be NULL.  Synchronous. */
+sph_status sph_hseed_norm(sph_ctx *ctx, float *get, const float *set);
 sph_status sph_hseed_get_stats(sph_ctx *ctx, sph_hseed_stats *out);
 
 /* FP64 conservation diagnostics (no counterpart in the reference, which

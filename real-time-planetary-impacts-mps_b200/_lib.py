@@ -39,6 +39,7 @@ FIELDS = {
     "grad_term": 8, "sound_speed": 9, "du": 10, "balsara": 11, "dhdt": 12, "grav_norm": 13,
     "material": 14, "active": 15, "next_active_time": 16, "global_time": 17, "dt": 18,
     "cell_key": 19, "cell_index": 20, "cell_start": 21, "cell_end": 22, "potential": 23, "pos64": 24,
+    "neighbours": 25,
 }
 VECTOR_FIELDS = ("pos", "vel", "acc")
 
@@ -194,6 +195,7 @@ def load(parity: bool = False) -> C.CDLL:
         "sph_hseed_gradient": (st, [vp, C.c_int32, C.c_uint32, _fp, _fp, vp]),
         "sph_hseed_params": (st, [vp, _fp, _fp]),
         "sph_hseed_dataset": (st, [vp, _fp, _fp, _fp]),
+        "sph_hseed_norm": (st, [vp, _fp, _fp]),
         "sph_hseed_get_stats": (st, [vp, C.POINTER(SphHSeedStats)]),
         "sph_draw_snapshot": (st, [vp, vp, _ip]),
         "sph_probe_fp32_fma": (st, [C.c_int32, C.c_int32, vp, vp]),

@@ -108,6 +108,7 @@ class Compute:
                     aneos_resolution, tree_source)
         s, keep = _ic_struct(ic)
         n = s.n
+        self._params_tuple = (max_children_in_leaf, max_tree_depth, max_unchecked_pointers, aneos_resolution)
         h = C.c_void_p()
         _lib.check(lib.sph_create(C.byref(p), C.byref(s), C.byref(h)), "sph_create", lib)
         self._lib = lib
@@ -267,6 +268,16 @@ class Compute:
         self._check(self._lib.sph_hseed_params(self._h, _ptr(out, _fp), None), "sph_hseed_params")
         return out
 
+    def hseed_norm(self, set_to=None) -> np.ndarray:
+        """The network's standardisation (18 floats; after setting it to
+        `set_to` when given)."""
+        if set_to is not None:
+            w = np.ascontiguousarray(np.asarray(set_to, np.float32))
+            self._check(self._lib.sph_hseed_norm(self._h, None, _ptr(w, _fp)), "sph_hseed_norm")
+        out = np.zeros(18, np.float32)
+        self._check(self._lib.sph_hseed_norm(self._h, _ptr(out, _fp), None), "sph_hseed_norm")
+        return out
+
     def hseed_dataset(self):
         """(features [n, 8], targets [n], standardisation [18]) of the recorded pass."""
         n = self.nParticles
@@ -389,6 +400,58 @@ class Compute:
 
     def clear_health(self):
         self._check(self._lib.sph_clear_health(self._h), "sph_clear_health")
+
+    # ---- checkpoint / resume (the reference has no resume) ----
+    CHECKPOINT_FIELDS = ("pos", "vel", "acc", "rho", "u", "mass", "pressure", "h", "grad_term", "sound_speed",
+                         "du", "balsara", "dhdt", "grav_norm", "material", "active", "next_active_time",
+                         "global_time", "dt")
+
+    def checkpoint(self, path: str):
+        """Write the whole simulation state to `path` (numpy .npz): every
+        per-particle field in the original order, the global time and dt,
+        the numerical form, the FP64 positions of the mixed form and the
+        learned seed's weights and standardisation (not its Adam moments, so
+        further training restarts them).  Synchronous.  resume() continues
+        from it with the same results as a run that was never stopped."""
+        self.synchronize()
+        out = {f: self.download(f) for f in self.CHECKPOINT_FIELDS}
+        form = self.get_form()
+        out["form"] = np.array([form["gravity"], str(form["theta"]), form["precision"], form["h_seed"],
+                                str(form["h_tolerance"])])
+        out["tree_source"] = np.array([self.tree_source])
+        out["params"] = np.array(self._params_tuple, np.int64)
+        if form["precision"] == "mixed":
+            out["pos64"] = self.download("pos64")
+        if form["h_seed"] == "learned":
+            out["hseed_params"] = self.hseed_params()
+            out["hseed_norm"] = self.hseed_norm()
+            out["neighbours"] = self.download("neighbours")
+        np.savez(path, **out)
+
+    @classmethod
+    def resume(cls, path: str, *, forsterite_table: str | None = None, fe85si15_table: str | None = None,
+               parity: bool = False) -> "Compute":
+        """A context in the state written by checkpoint(path)."""
+        with np.load(path) as z:
+            ck = {k: z[k] for k in z.files}
+        leaf, depth, unchecked, res = (int(v) for v in ck["params"])
+        ic = {k: ck[k] for k in ("pos", "vel", "rho", "u", "mass", "pressure", "h", "material")}
+        c = cls(ic, max_children_in_leaf=leaf, max_tree_depth=depth, max_unchecked_pointers=unchecked,
+                aneos_resolution=res, tree_source=str(ck["tree_source"][0]), forsterite_table=forsterite_table,
+                fe85si15_table=fe85si15_table, parity=parity)
+        g, th, prec, seed, tol = (str(v) for v in ck["form"])
+        if "hseed_params" in ck:
+            c.hseed_params(ck["hseed_params"])
+            c.hseed_norm(ck["hseed_norm"])
+            c.upload("neighbours", ck["neighbours"])
+        c.set_form(gravity=g, theta=float(th), precision=prec, h_seed=seed, h_tolerance=float(tol))
+        for f in cls.CHECKPOINT_FIELDS:
+            if f not in ic:
+                c.upload(f, ck[f])
+        if "pos64" in ck:
+            c.upload("pos64", ck["pos64"])
+        c.synchronize()
+        return c
 
     def state(self) -> dict:
         names = ("pos", "vel", "acc", "rho", "u", "mass", "pressure", "h", "grad_term", "sound_speed", "du",

@@ -540,15 +540,26 @@ sph_status sph_upload_async(sph_ctx *ctx, sph_field field, const void *host, siz
         case SPH_FIELD_MATERIAL: return f1(ctx->mat, 4);
         case SPH_FIELD_ACTIVE: return f1(ctx->active, 1);
         case SPH_FIELD_NEXT_ACTIVE: return f1(ctx->nat, 4);
+        case SPH_FIELD_NEIGHBOURS: {
+            sph_status s = hseed_alloc(ctx);
+            if (s != SPH_OK) return s;
+            return f1(ctx->hs.nn, 4);
+        }
         case SPH_FIELD_GLOBAL_TIME:
-        case SPH_FIELD_DT:
+        case SPH_FIELD_DT: {
             if (count != 1) {
                 set_error("sph_upload: scalar field expects 1 element");
                 return SPH_ERR_INVALID_ARG;
             }
-            return cuda_status(cudaMemcpyAsync(ctx->globals + (field == SPH_FIELD_DT ? 1 : 0), host, 4,
-                                               cudaMemcpyHostToDevice, st),
-                               "sph_upload");
+            cudaError_t e = cudaMemcpyAsync(ctx->globals + (field == SPH_FIELD_DT ? 1 : 0), host, 4,
+                                            cudaMemcpyHostToDevice, st);
+            // the mixed form's FP64 time follows (ticks x 2^-11 s is exact in FP64)
+            if (e == cudaSuccess && field == SPH_FIELD_GLOBAL_TIME && ctx->form.precision == SPH_PRECISION_MIXED) {
+                k_time_to64<<<1, 1, 0, st>>>(ctx->globals, ctx->dglob);
+                e = cudaGetLastError();
+            }
+            return cuda_status(e, "sph_upload");
+        }
         default:
             set_error("sph_upload: field %d is read-only", (int)field);
             return SPH_ERR_INVALID_ARG;
@@ -624,6 +635,12 @@ sph_status sph_download_async(sph_ctx *ctx, sph_field field, void *host, size_t 
         case SPH_FIELD_DHDT: return f1(ctx->dhdt, 4, n);
         case SPH_FIELD_GRAV_NORM: return f1(ctx->gnorm, 4, n);
         case SPH_FIELD_POTENTIAL: return f1(ctx->phi, 4, n);
+        case SPH_FIELD_NEIGHBOURS:
+            if (!ctx->hs.nn) {
+                set_error("sph_download: no neighbour counts (the learned h seed is not in use)");
+                return SPH_ERR_INVALID_ARG;
+            }
+            return f1(ctx->hs.nn, 4, n);
         case SPH_FIELD_MATERIAL: return f1(ctx->mat, 4, n);
         case SPH_FIELD_ACTIVE: return f1(ctx->active, 1, n);
         case SPH_FIELD_NEXT_ACTIVE: return f1(ctx->nat, 4, n);
@@ -690,6 +707,7 @@ sph_status sph_get_buffer(sph_ctx *ctx, sph_field field, void **device_ptr, size
         case SPH_FIELD_CELL_START: p = ctx->cell_range; b = 8 * (size_t)kNumCells; s = 8; break;
         case SPH_FIELD_CELL_END: p = (char *)ctx->cell_range + 4; b = 8 * (size_t)kNumCells; s = 8; break;
         case SPH_FIELD_POS64: p = ctx->pos64; b = 32 * n; s = 32; break;
+        case SPH_FIELD_NEIGHBOURS: p = ctx->hs.nn; b = 4 * n; break;
         default: return SPH_ERR_INVALID_ARG;
     }
     *device_ptr = p;

@@ -623,6 +623,24 @@ sph_status sph_hseed_params(sph_ctx *ctx, float *get, const float *set) {
     return cuda_status(e, "sph_hseed_params");
 }
 
+sph_status sph_hseed_norm(sph_ctx *ctx, float *get, const float *set) {
+    if (!ctx) return SPH_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    sph_status s = hseed_alloc(ctx);
+    if (s != SPH_OK) return s;
+    if (get && !ctx->hs.have_norm) {
+        set_error("sph_hseed_norm: no standardisation yet (sph_hseed_train computes it)");
+        return SPH_ERR_INVALID_ARG;
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && get) e = cudaMemcpy(get, ctx->hs.norm, sizeof(float) * kNorm, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && set) {
+        e = cudaMemcpy(ctx->hs.norm, set, sizeof(float) * kNorm, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) ctx->hs.have_norm = true;
+    }
+    return cuda_status(e, "sph_hseed_norm");
+}
+
 sph_status sph_hseed_dataset(sph_ctx *ctx, float *features, float *targets, float *norm) {
     if (!ctx) return SPH_ERR_INVALID_ARG;
     if (!ctx->hs.have_data) {
