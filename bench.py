@@ -58,8 +58,8 @@ PASS_KERNELS = {
     "tree": "k_bbox, k_tree_keys, k_onesweep x3, k_children/k_emit/scan x7, k_marks, k_write, k_link",
     "sort": "k_hash_hist, k_onesweep x3, k_cells",
     "gravity": "plain: k_up x8, k_down x8; chosen: k_up_theta x8, k_gather_key_order, k_walk",
-    "density": "k_gather, [k_mlp (learned seed)], k_density",
-    "acceleration": "k_acceleration",
+    "density": "k_gather, [k_mlp (learned seed)], k_tile_starts, k_density_tile, k_density_deferred",
+    "acceleration": "k_tile_starts, k_acceleration_tile, k_acceleration_deferred",
     "step": "k_step",
 }
 
@@ -70,8 +70,9 @@ def launches_per_step(depth: int, chosen: bool) -> int:
     tree = 3 + 3 + 1 + depth * (1 + scan + 1) + 1 + 1 + (depth + 1) + 2 * scan + (depth + 1) + depth
     sort = 1 + 3 + 1
     gravity = (depth + 1) + 2 if chosen else 2 * (depth + 1)
-    density = 2 + (1 if chosen else 0)
-    return tree + sort + gravity + density + 1 + 1
+    density = 4 + (1 if chosen else 0)   # gather, tile starts, tile pass, deferred pass [, seed]
+    acceleration = 3                     # tile starts, tile pass, deferred pass
+    return tree + sort + gravity + density + acceleration + 1
 
 
 def load_peaks() -> dict:
@@ -605,6 +606,8 @@ def main():
                         "plain": {p: round(v, 4) for p, v in pp.items()}},
             "h_seed": {"sweeps_per_particle": sweeps, "max_sweeps": st["max_sweeps"],
                        "fallback_rate": st["fallbacks"] / max(st["particles"], 1),
+                       "density_tiles": st["tiles"], "density_deferred_particles": st["deferred"],
+                       "acceleration_deferred_particles": st["accel_deferred"],
                        "training_ms_per_call": float(np.mean(train_ms)), "adam_steps_per_call": args.train_iters},
             "roofline": {"bound": "hbm", "kernel": f"{dom} pass ({PASS_KERNELS[dom]}), chosen form",
                          "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",

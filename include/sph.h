@@ -216,6 +216,7 @@ typedef struct {
     uint32_t particles;  /* particles iterated */
     uint32_t tiles;      /* occupied cell octets the product build's density pass staged */
     uint32_t deferred;   /* particles it handed from the tiles to the per-particle walk */
+    uint32_t accel_deferred; /* the same count of the last acceleration pass */
 } sph_hseed_stats;
 int32_t sph_hseed_num_params(void);
 sph_status sph_hseed_capture(sph_ctx *ctx, int32_t on);

@@ -119,6 +119,7 @@ def load(kind: str = "oracle") -> C.CDLL:
         lib.ref_tree_free.argtypes = [vp]
         lib.ref_aneos_load.argtypes = [C.c_char_p, C.c_int, _fp]
         lib.ref_aneos_load.restype = C.c_int
+        lib.ref_draw_snapshot.argtypes = [C.c_int, _fp, _ip, _ip]
     else:
         raise ValueError(kind)
     _LIBS[kind] = lib
@@ -293,6 +294,35 @@ class OracleState:
         for k in ("material", "active", "next_active_time", "global_time", "dt", "cell_key", "cell_index"):
             out[k] = getattr(self, k).copy()
         return out
+
+
+def draw_snapshot(pos: np.ndarray, material: np.ndarray) -> np.ndarray:
+    """render.metal:49-66 restated in numpy: each particle's (x, y) shifted
+    by -250 Mm and scaled by 1024 / (20 R_E) in float32; inside [0, 1024] it
+    takes pixel int(u) + (1023 - int(v)) * 1024 and the image keeps the
+    largest material id per pixel.  Splats at exactly 1024 (one past the
+    image in the reference) are dropped."""
+    p = np.asarray(pos, np.float32).reshape(-1, 3)
+    R_E = np.float32(6.3710)
+    s = np.float32(1024) / (np.float32(20) * R_E)
+    ux = (p[:, 0] - np.float32(250)) * s
+    uy = (p[:, 1] - np.float32(250)) * s
+    ok = (ux >= 0) & (uy >= 0) & (ux < 1024) & (uy < 1024)
+    px = ux[ok].astype(np.int64) + (1023 - uy[ok].astype(np.int64)) * 1024
+    img = np.zeros(1024 * 1024, np.int64)
+    np.maximum.at(img, px, np.asarray(material).reshape(-1)[ok].astype(np.int64))
+    return img.astype(np.int32).reshape(1024, 1024)
+
+
+def draw_snapshot_ref(pos: np.ndarray, material: np.ndarray) -> np.ndarray:
+    """The reference's drawToSnapshot (render.metal:49-66) over all
+    particles into a cleared 1024 x 1024 int image (oracle/_ref)."""
+    lib = load("ref")
+    pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    mat = np.ascontiguousarray(material, np.int32).reshape(-1)
+    img = np.zeros((1024, 1024), np.int32)
+    lib.ref_draw_snapshot(pos.shape[0], ptr(pos, _fp), ptr(mat, _ip), ptr(img, _ip))
+    return img
 
 
 def last_tree_nodes(n_nodes: int):

@@ -18,7 +18,7 @@ MSL=(-x c++ -fsingle-precision-constant -Wno-attributes -I "$HERE/ref_shim" -I "
 objs=()
 for f in sort density accelerations step gravity/gravity gravity/poles/P2M gravity/poles/M2M \
          gravity/poles/M2L gravity/poles/L2L gravity/poles/L2P gravity/poles/derivatives \
-         gravity/poles/accept gravity/poles/helpers; do
+         gravity/poles/accept gravity/poles/helpers render; do
   o="$OBJ/$(echo "$f" | tr '/' '_').o"
   "$CXX" "${COMMON[@]}" "${MSL[@]}" -c "$SH/$f.metal" -o "$o"
   objs+=("$o")

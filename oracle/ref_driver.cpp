@@ -40,6 +40,7 @@ void density(float3 *, float3 *, float *, float *, float *, float *, float *, in
 void acceleration(float3 *, float3 *, float3 *, float *, float *, float *, float *, float *, float *, float *, float *,
                   float *, float *, uint2 *, int *, int *, float *, int *, bool *, int *, int *, atomic_int *, uint);
 void step(float3 *, float3 *, float3 *, float *, float *, float *, float *, float *, bool *, int *, int *, int *, uint);
+void drawToSnapshot(float3 *, int *, atomic_int *, uint);  // render.metal:49-66
 
 // ---- reference host routines (octree.cpp, ANEOS.cpp) ------------------------
 #include <vector>
@@ -245,6 +246,16 @@ void ref_tree_export(const ref_tree *t, int32_t *tree, int32_t *off, int32_t *no
     off[t->levels.size()] = o;
 }
 void ref_tree_free(ref_tree *t) { delete t; }
+
+// Compute::drawSnapshot (Compute.cpp:395-412): clear the image, then the
+// reference's drawToSnapshot kernel for every particle
+void ref_draw_snapshot(int n, const float *pos3, const int *mat, int *img) {
+    std::vector<float3> p = to3(pos3, n);
+    std::vector<int> m(mat, mat + n);
+    for (size_t i = 0; i < (size_t)1024 * 1024; ++i) img[i] = 0;
+    atomic_int *out = reinterpret_cast<atomic_int *>(img);
+    for (int i = 0; i < n; ++i) drawToSnapshot(p.data(), m.data(), out, (uint)i);
+}
 
 // ANEOS.cpp:21-175
 int ref_aneos_load(const char *path, int res, float *out) {

@@ -83,7 +83,8 @@ class SphEnsembleTuning(C.Structure):
 
 class SphHSeedStats(C.Structure):
     _fields_ = [("sweeps", C.c_uint32), ("fallbacks", C.c_uint32), ("max_sweeps", C.c_uint32),
-                ("particles", C.c_uint32), ("tiles", C.c_uint32), ("deferred", C.c_uint32)]
+                ("particles", C.c_uint32), ("tiles", C.c_uint32), ("deferred", C.c_uint32),
+                ("accel_deferred", C.c_uint32)]
 
 
 SPH_HSEED_PLAIN = 0

@@ -293,7 +293,7 @@ class Compute:
         st = _lib.SphHSeedStats()
         self._check(self._lib.sph_hseed_get_stats(self._h, C.byref(st)), "sph_hseed_get_stats")
         return dict(sweeps=st.sweeps, fallbacks=st.fallbacks, max_sweeps=st.max_sweeps, particles=st.particles,
-                    tiles=st.tiles, deferred=st.deferred)
+                    tiles=st.tiles, deferred=st.deferred, accel_deferred=st.accel_deferred)
 
     def diagnostics(self, stream=None, theta_potential: float = 0.5) -> dict:
         """FP64 conservation sums (mass, energies, momentum, angular momentum)."""

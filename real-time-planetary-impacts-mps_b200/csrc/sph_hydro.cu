@@ -259,6 +259,7 @@ __device__ __forceinline__ int group_collect(float px, float py, float pz, float
 struct DensityArgs {
     int n;
     const uint32_t *cidx;
+    const uint32_t *skey;  // sorted cell keys (tile passes)
     const uint2 *cells;
     const float4 *sp4, *sv4;
     float *h, *rho, *f, *P, *c, *B;
@@ -562,13 +563,27 @@ __global__ void __launch_bounds__(parts_per_block<L>() * L)
 // k_density_deferred, which runs the per-particle walk above; so is every
 // particle of a tile whose box exceeds the shared-memory budget.
 constexpr int kTileThreads = 384;
-constexpr int kTileLanes = 8;                               // lanes per particle
+#ifndef SPH_TILE_LANES
+#define SPH_TILE_LANES 8
+#endif
+constexpr int kTileLanes = SPH_TILE_LANES;                  // lanes per particle
+constexpr int kTileGpw = 32 / kTileLanes;                   // particles per warp
 constexpr int kTileGroups = kTileThreads / kTileLanes;      // particles in flight per CTA
 constexpr int kTileStageMax = 3840;                         // staged particles per tile
 constexpr int kTileCellsMax = 1024;                         // cells of a tile's staged box
 constexpr int kTileCellsPerThread = (kTileCellsMax + kTileThreads - 1) / kTileThreads;
 constexpr int kTileReach = 3;                               // cells a list box may extend past its own cell
 constexpr int kTileList = 256;                              // list entries per particle (staged slots)
+#ifndef SPH_TILE_LIST_REACH
+#define SPH_TILE_LIST_REACH 1.05f
+#endif
+constexpr float kTileListReach = SPH_TILE_LIST_REACH;       // list radius / (2 h)
+#ifndef SPH_TILE_STAGE_REACH
+#define SPH_TILE_STAGE_REACH 1.15f
+#endif
+// staged box radius / (2 h): room for h to grow before a list rebuild leaves
+// the staged box
+constexpr float kTileStageReach = SPH_TILE_STAGE_REACH;
 
 struct TileShared {
     float4 pos[kTileStageMax];          // staged (x, y, z, m)
@@ -584,14 +599,15 @@ struct TileShared {
 };
 
 // The list box of a tile particle at smoothing length hb -- the cells within
-// 2 hb kListReach, widened by 1e-3 of a cell so that float rounding of the
+// 2 hb kTileListReach, widened by 1e-3 of a cell so that float rounding of the
 // cell coordinates (|x| / CELL_WIDTH < 2^12, a few 1e-4 of a cell) never drops
 // a cell -- and whether the tile path can take the particle (reach within
 // kTileReach cells of its own, h < MAX_H).
-__device__ __forceinline__ bool tile_box(float px, float py, float pz, float hb, CellBox &b) {
+__device__ __forceinline__ bool tile_box(float px, float py, float pz, float hb, CellBox &b,
+                                         float reach = kTileListReach) {
     constexpr float iw = 1.f / kCellWidth;
     constexpr float widen = 1e-3f;
-    const float rl = 2.f * hb * kListReach;
+    const float rl = 2.f * hb * reach;
     b.lo0 = (int)floorf((px - rl) * iw - widen);
     b.lo1 = (int)floorf((py - rl) * iw - widen);
     b.lo2 = (int)floorf((pz - rl) * iw - widen);
@@ -729,7 +745,7 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, TileShar
     }
     const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
     const int ny = S.box[4] - lo1 + 1, nz = S.box[5] - lo2 + 1;
-    // the group's list: staged slots within 2 hb kListReach
+    // the group's list: staged slots within 2 hb kTileListReach
     int n_list = -1;
     float list_r2 = 0.f;
     auto build = [&](bool want, float hb) {
@@ -745,22 +761,22 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, TileShar
             b.lo0 = b.lo1 = b.lo2 = kBig;
             b.hi0 = b.hi1 = b.hi2 = -kBig;
         }
-        const float rl = 2.f * hb * kListReach;
+        const float rl = 2.f * hb * kTileListReach;
         const float r2 = want ? rl * rl : -1.f;
         const int u0 = __reduce_min_sync(kFull, b.lo0), u1 = __reduce_min_sync(kFull, b.lo1),
                   u2 = __reduce_min_sync(kFull, b.lo2);
         const int v0 = __reduce_max_sync(kFull, b.hi0), v1 = __reduce_max_sync(kFull, b.hi1),
                   v2 = __reduce_max_sync(kFull, b.hi2);
         if (u0 > v0) return;  // no group builds
-        float qx[4], qy[4], qz[4], qr[4];
+        float qx[kTileGpw], qy[kTileGpw], qz[kTileGpw], qr[kTileGpw];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < kTileGpw; ++k) {
             qx[k] = __shfl_sync(kFull, px, k * L);
             qy[k] = __shfl_sync(kFull, py, k * L);
             qz[k] = __shfl_sync(kFull, pz, k * L);
             qr[k] = __shfl_sync(kFull, r2, k * L);
         }
-        int cnt[4] = {0, 0, 0, 0};
+        int cnt[kTileGpw] = {};
         const unsigned below = (1u << lane) - 1u;
         constexpr float w = kCellWidth;
         constexpr float iw = 1.f / kCellWidth;
@@ -777,7 +793,7 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, TileShar
                 const int x = u0 + r / nyu, y = u1 + r % nyu;
                 int zl = 0x3fffffff, zh = -0x3fffffff;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < kTileGpw; ++k) {
                     const float gx = fmaxf(fmaxf((float)x * w - qx[k], qx[k] - (float)(x + 1) * w) - kCellMargin, 0.f);
                     const float gy = fmaxf(fmaxf((float)y * w - qy[k], qy[k] - (float)(y + 1) * w) - kCellMargin, 0.f);
                     const float g2 = gx * gx + gy * gy;
@@ -816,7 +832,7 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, TileShar
                 const uint32_t s = sj + (v - ej);
                 if (v < total) q = S.pos[s];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < kTileGpw; ++k) {
                     const float dx = q.x - qx[k], dy = q.y - qy[k], dz = q.z - qz[k];
                     const bool hit = dx * dx + dy * dy + dz * dz <= qr[k];
                     const unsigned bal = __ballot_sync(kFull, hit);
@@ -830,7 +846,10 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, TileShar
         }
         __syncwarp();
         if (want) {
-            const int c = g == 0 ? cnt[0] : g == 1 ? cnt[1] : g == 2 ? cnt[2] : cnt[3];
+            int c = 0;
+#pragma unroll
+            for (int k = 0; k < kTileGpw; ++k)
+                if (g == k) c = cnt[k];
             if (c > kTileList) {
                 defer();
             } else {
@@ -992,121 +1011,150 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 S.start = r.x;
                 S.end = r.y;
             }
-            S.next = 0u;
-            S.box[0] = S.box[1] = S.box[2] = 0x7fffffff;
-            S.box[3] = S.box[4] = S.box[5] = -0x7fffffff;
-            S.defer_all = 0;
         }
         __syncthreads();
         if (S.tile >= ntiles) break;
-        const uint32_t start = S.start, end = S.end;
-        // the staged box: union of the list boxes of the tile's active particles
-        {
-            int b[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, -0x7fffffff, -0x7fffffff, -0x7fffffff};
-            for (uint32_t p = start + tid; p < end; p += kTileThreads) {
-                const uint32_t ind = a.cidx[p];
-                if (!a.active[ind]) continue;
-                const float4 me = a.sp4[p];
-                const float h_plain = a.h[ind];
-                bool seeded;
-                const float h0 = tile_start_h(a, ind, h_plain, seeded);
-                CellBox cb;
-                if (!tile_box(me.x, me.y, me.z, fmaxf(h0, h_plain), cb)) continue;
-                b[0] = min(b[0], cb.lo0);
-                b[1] = min(b[1], cb.lo1);
-                b[2] = min(b[2], cb.lo2);
-                b[3] = max(b[3], cb.hi0);
-                b[4] = max(b[4], cb.hi1);
-                b[5] = max(b[5], cb.hi2);
+        const uint32_t tstart = S.start, tend = S.end;
+        // a tile whose staged box overflows shared memory is taken again as
+        // its octets, one at a time; an octet that still overflows is handed
+        // to the per-particle pass
+        const bool splittable = (a.skey[tstart] >> 3) != (a.skey[tend - 1] >> 3);
+        bool whole = true;
+        uint32_t r0 = tstart;
+        while (r0 < tend) {
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t r1 = tend;
+                if (!whole) {  // the rest of r0's octet
+                    const uint32_t o = a.skey[r0] >> 3;
+                    r1 = r0 + 1u;
+                    for (int j = 0; j < 8; ++j) {
+                        const uint2 r = a.cells[o * 8u + (uint32_t)j];
+                        if (r.x != 0xffffffffu) r1 = max(r1, r.y + 1u);
+                    }
+                }
+                S.end = r1;
+                S.next = 0u;
+                S.box[0] = S.box[1] = S.box[2] = 0x7fffffff;
+                S.box[3] = S.box[4] = S.box[5] = -0x7fffffff;
+                S.defer_all = 0;
             }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                b[k] = __reduce_min_sync(0xffffffffu, b[k]);
-                b[k + 3] = __reduce_max_sync(0xffffffffu, b[k + 3]);
-            }
-            if (lane == 0) {
-#pragma unroll
+            __syncthreads();
+            const uint32_t start = r0, end = S.end;
+            // the staged box: union of the list boxes of the tile's active particles
+            {
+                int b[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, -0x7fffffff, -0x7fffffff, -0x7fffffff};
+                for (uint32_t p = start + tid; p < end; p += kTileThreads) {
+                    const uint32_t ind = a.cidx[p];
+                    if (!a.active[ind]) continue;
+                    const float4 me = a.sp4[p];
+                    const float h_plain = a.h[ind];
+                    bool seeded;
+                    const float h0 = tile_start_h(a, ind, h_plain, seeded);
+                    CellBox cb;
+                    if (!tile_box(me.x, me.y, me.z, fmaxf(h0, h_plain), cb)) continue;
+                    tile_box(me.x, me.y, me.z, fmaxf(h0, h_plain), cb, fmaxf(kTileStageReach, kTileListReach));
+                    b[0] = min(b[0], cb.lo0);
+                    b[1] = min(b[1], cb.lo1);
+                    b[2] = min(b[2], cb.lo2);
+                    b[3] = max(b[3], cb.hi0);
+                    b[4] = max(b[4], cb.hi1);
+                    b[5] = max(b[5], cb.hi2);
+                }
+    #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    atomicMin(&S.box[k], b[k]);
-                    atomicMax(&S.box[k + 3], b[k + 3]);
+                    b[k] = __reduce_min_sync(0xffffffffu, b[k]);
+                    b[k + 3] = __reduce_max_sync(0xffffffffu, b[k + 3]);
+                }
+                if (lane == 0) {
+    #pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        atomicMin(&S.box[k], b[k]);
+                        atomicMax(&S.box[k + 3], b[k + 3]);
+                    }
                 }
             }
-        }
-        __syncthreads();
-        const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
-        const bool any = lo0 <= S.box[3];  // some particle of the tile takes the tile path
-        const int nx = any ? S.box[3] - lo0 + 1 : 0, ny = any ? S.box[4] - lo1 + 1 : 0,
-                  nz = any ? S.box[5] - lo2 + 1 : 0;
-        int ncell = 0;
-        if (any) {
-            if (nx * ny * nz > kTileCellsMax) {
-                if (tid == 0) S.defer_all = 1;
-            } else {
-                ncell = nx * ny * nz;
-            }
-        }
-        // cell counts (kTileCellsPerThread consecutive cells per thread) and
-        // their exclusive scan
-        uint32_t c_cnt[kTileCellsPerThread];
-        uint32_t tsum = 0u;
-#pragma unroll
-        for (int k = 0; k < kTileCellsPerThread; ++k) {
-            const int c = kTileCellsPerThread * tid + k;
-            c_cnt[k] = 0u;
-            if (c < ncell) {
-                const int ix = c / (ny * nz), rem = c - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
-                const uint2 r = __ldg(a.cells + cell_index_of(lo0 + ix, lo1 + iy, lo2 + iz));
-                if (r.x != 0xffffffffu) {
-                    c_cnt[k] = r.y - r.x + 1u;
-                    S.first[c] = r.x;
+            __syncthreads();
+            const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
+            const bool any = lo0 <= S.box[3];  // some particle of the tile takes the tile path
+            const int nx = any ? S.box[3] - lo0 + 1 : 0, ny = any ? S.box[4] - lo1 + 1 : 0,
+                      nz = any ? S.box[5] - lo2 + 1 : 0;
+            int ncell = 0;
+            if (any) {
+                if (nx * ny * nz > kTileCellsMax) {
+                    if (tid == 0) S.defer_all = 1;
+                } else {
+                    ncell = nx * ny * nz;
                 }
             }
-            tsum += c_cnt[k];
-        }
-        uint32_t inc = tsum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        if (lane == 31) S.wsum[tid >> 5] = inc;
-        __syncthreads();
-        uint32_t wbase = 0u;
-        for (int w = 0; w < (tid >> 5); ++w) wbase += S.wsum[w];
-        uint32_t run = wbase + inc - tsum;
-#pragma unroll
-        for (int k = 0; k < kTileCellsPerThread; ++k) {
-            const int c = kTileCellsPerThread * tid + k;
-            if (c < ncell) S.off[c] = run;
-            run += c_cnt[k];
-        }
-        if (tid == kTileThreads - 1) {
-            S.off[ncell] = run;
-            if (run > (uint32_t)kTileStageMax) S.defer_all = 1;
-        }
-        __syncthreads();
-        if (!S.defer_all) {
-            const uint32_t total = S.off[ncell];
-            for (uint32_t s = tid; s < total; s += kTileThreads) {
-                int lo = 0, hi = ncell - 1;  // the last cell whose first slot is <= s
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (S.off[mid] <= s) lo = mid;
-                    else hi = mid - 1;
+            // cell counts (kTileCellsPerThread consecutive cells per thread) and
+            // their exclusive scan
+            uint32_t c_cnt[kTileCellsPerThread];
+            uint32_t tsum = 0u;
+    #pragma unroll
+            for (int k = 0; k < kTileCellsPerThread; ++k) {
+                const int c = kTileCellsPerThread * tid + k;
+                c_cnt[k] = 0u;
+                if (c < ncell) {
+                    const int ix = c / (ny * nz), rem = c - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
+                    const uint2 r = __ldg(a.cells + cell_index_of(lo0 + ix, lo1 + iy, lo2 + iz));
+                    if (r.x != 0xffffffffu) {
+                        c_cnt[k] = r.y - r.x + 1u;
+                        S.first[c] = r.x;
+                    }
                 }
-                const uint32_t g = S.first[lo] + (s - S.off[lo]);
-                S.pos[s] = __ldg(a.sp4 + g);
-                S.gidx[s] = g;
+                tsum += c_cnt[k];
             }
-        }
-        __syncthreads();
-        // warps take the tile's particles four at a time
-        for (;;) {
-            uint32_t j = 0u;
-            if (lane == 0) j = atomicAdd(&S.next, 4u);
-            j = __shfl_sync(0xffffffffu, j, 0);
-            if (start + j >= end) break;
-            density_tile_warp(a, S, start + j, end, lane, &S.list[(tid >> 5) * 4], deferred, ctr + 2);
+            uint32_t inc = tsum;
+    #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            if (lane == 31) S.wsum[tid >> 5] = inc;
+            __syncthreads();
+            uint32_t wbase = 0u;
+            for (int w = 0; w < (tid >> 5); ++w) wbase += S.wsum[w];
+            uint32_t run = wbase + inc - tsum;
+    #pragma unroll
+            for (int k = 0; k < kTileCellsPerThread; ++k) {
+                const int c = kTileCellsPerThread * tid + k;
+                if (c < ncell) S.off[c] = run;
+                run += c_cnt[k];
+            }
+            if (tid == kTileThreads - 1) {
+                S.off[ncell] = run;
+                if (run > (uint32_t)kTileStageMax) S.defer_all = 1;
+            }
+            __syncthreads();
+            if (S.defer_all && whole && splittable) {
+                whole = false;
+                continue;
+            }
+            if (!S.defer_all) {
+                const uint32_t total = S.off[ncell];
+                for (uint32_t s = tid; s < total; s += kTileThreads) {
+                    int lo = 0, hi = ncell - 1;  // the last cell whose first slot is <= s
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (S.off[mid] <= s) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    const uint32_t g = S.first[lo] + (s - S.off[lo]);
+                    S.pos[s] = __ldg(a.sp4 + g);
+                    S.gidx[s] = g;
+                }
+            }
+            __syncthreads();
+            // warps take the tile's particles four at a time
+            for (;;) {
+                uint32_t j = 0u;
+                if (lane == 0) j = atomicAdd(&S.next, (uint32_t)kTileGpw);
+                j = __shfl_sync(0xffffffffu, j, 0);
+                if (start + j >= end) break;
+                density_tile_warp(a, S, start + j, end, lane, &S.list[(tid >> 5) * kTileGpw], deferred, ctr + 2);
+            }
+            r0 = end;
         }
     }
     if (a.stats && tid == 0) {
@@ -1122,6 +1170,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 struct AccelArgs {
     int n;
     const uint32_t *cidx;
+    const uint32_t *skey;  // sorted cell keys (tile passes)
     const uint2 *cells;
     const float4 *sA, *sB, *sC;
     float4 *acc4;
@@ -1385,7 +1434,7 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
     constexpr unsigned kFull = 0xffffffffu;
     constexpr int kBig = 0x3fffffff;
     const int g = lane / L, sub = lane & (L - 1);
-    uint16_t *list = S.list[wslot * 4 + g];
+    uint16_t *list = S.list[wslot * kTileGpw + g];
     const uint32_t p = p0 + (uint32_t)g;
     bool live = p < end;
     uint32_t ind = 0u;
@@ -1417,7 +1466,7 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
         b.hi0 = b.hi1 = b.hi2 = -kBig;
     }
     if (want && sub == 0) {
-        int *gb = S.gbox[wslot * 4 + g];
+        int *gb = S.gbox[wslot * kTileGpw + g];
         gb[0] = b.lo0 - lo0;
         gb[1] = b.lo1 - lo1;
         gb[2] = b.lo2 - lo2;
@@ -1433,9 +1482,9 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
     __syncwarp();
     // every accepted pair lies within 2 max(h_i, largest staged h) of the particle
     const float hm = fmaxf(I.hi, __int_as_float(S.hmax_bits));
-    float qx[4], qy[4], qz[4], qr[4], qR[4];
+    float qx[kTileGpw], qy[kTileGpw], qz[kTileGpw], qr[kTileGpw], qR[kTileGpw];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < kTileGpw; ++k) {
         qx[k] = __shfl_sync(kFull, I.xi, k * L);
         qy[k] = __shfl_sync(kFull, I.yi, k * L);
         qz[k] = __shfl_sync(kFull, I.zi, k * L);
@@ -1443,7 +1492,7 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
         qR[k] = __shfl_sync(kFull, want ? 4.f * hm * hm : -1.f, k * L);
     }
     // box bounds of the four groups, for the row test (lane k * L holds group k's)
-    int cnt[4] = {0, 0, 0, 0};
+    int cnt[kTileGpw] = {};
     const unsigned below = (1u << lane) - 1u;
     const int nyu = v1 - u1 + 1;
     const int rows = (v0 - u0 + 1) * nyu;
@@ -1461,7 +1510,7 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
         constexpr float w = kCellWidth;
         constexpr float iw = 1.f / kCellWidth;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < kTileGpw; ++k) {
             const int bl0 = __shfl_sync(kFull, b.lo0, k * L), bh0 = __shfl_sync(kFull, b.hi0, k * L);
             const int bl1 = __shfl_sync(kFull, b.lo1, k * L), bh1 = __shfl_sync(kFull, b.hi1, k * L);
             const int bl2 = __shfl_sync(kFull, b.lo2, k * L), bh2 = __shfl_sync(kFull, b.hi2, k * L);
@@ -1507,7 +1556,7 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
             }
             const float hj2x4 = q.w * q.w * 4.f;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < kTileGpw; ++k) {
                 const float dx = qx[k] - q.x, dy = qy[k] - q.y, dz = qz[k] - q.z;
                 const float r2 = dx * dx + dy * dy + dz * dz;
                 const bool near = r2 >= 1e-12f;
@@ -1515,7 +1564,7 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
                 // r > 2 h_i but r <= 2 h_j: only when the neighbour's cell is in the box
                 const bool maybe = near && !hit && qr[k] >= 0.f && r2 <= hj2x4;
                 if (__any_sync(kFull, maybe)) {
-                    const int *gb = S.gbox[wslot * 4 + k];
+                    const int *gb = S.gbox[wslot * kTileGpw + k];
                     const int cx = (int)(sc & 1023u), cy = (int)((sc >> 10) & 1023u), cz = (int)(sc >> 20);
                     if (maybe && cx >= gb[0] && cx <= gb[3] && cy >= gb[1] && cy <= gb[4] && cz >= gb[2] &&
                         cz <= gb[5])
@@ -1524,14 +1573,17 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
                 const unsigned bal = __ballot_sync(kFull, hit);
                 if (hit) {
                     const int at = cnt[k] + __popc(bal & below);
-                    if (at < kTileList) S.list[wslot * 4 + k][at] = (uint16_t)s;
+                    if (at < kTileList) S.list[wslot * kTileGpw + k][at] = (uint16_t)s;
                 }
                 cnt[k] += __popc(bal);
             }
         }
     }
     __syncwarp();
-    const int n_list = g == 0 ? cnt[0] : g == 1 ? cnt[1] : g == 2 ? cnt[2] : cnt[3];
+    int n_list = 0;
+#pragma unroll
+    for (int k = 0; k < kTileGpw; ++k)
+        if (g == k) n_list = cnt[k];
     if (live && n_list > kTileList) {
         if (sub == 0) deferred[atomicAdd(dctr, 1u)] = p;
         live = false;
@@ -1573,128 +1625,156 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 S.start = r.x;
                 S.end = r.y;
             }
-            S.next = 0u;
-            S.box[0] = S.box[1] = S.box[2] = 0x7fffffff;
-            S.box[3] = S.box[4] = S.box[5] = -0x7fffffff;
-            S.defer_all = 0;
-            S.hmax_bits = 0;
         }
         __syncthreads();
         if (S.tile >= ntiles) break;
-        const uint32_t start = S.start, end = S.end;
-        {
-            int b[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, -0x7fffffff, -0x7fffffff, -0x7fffffff};
-            for (uint32_t p = start + tid; p < end; p += kTileThreads) {
-                if (!a.active[a.cidx[p]]) continue;
-                const float4 A = a.sA[p];
-                CellBox cb;
-                if (!accel_box(A.x, A.y, A.z, A.w, cb)) continue;
-                b[0] = min(b[0], cb.lo0);
-                b[1] = min(b[1], cb.lo1);
-                b[2] = min(b[2], cb.lo2);
-                b[3] = max(b[3], cb.hi0);
-                b[4] = max(b[4], cb.hi1);
-                b[5] = max(b[5], cb.hi2);
+        const uint32_t tstart = S.start, tend = S.end;
+        // a tile whose staged box overflows shared memory is taken again as
+        // its octets, one at a time; an octet that still overflows is handed
+        // to the per-particle pass
+        const bool splittable = (a.skey[tstart] >> 3) != (a.skey[tend - 1] >> 3);
+        bool whole = true;
+        uint32_t r0 = tstart;
+        while (r0 < tend) {
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t r1 = tend;
+                if (!whole) {  // the rest of r0's octet
+                    const uint32_t o = a.skey[r0] >> 3;
+                    r1 = r0 + 1u;
+                    for (int j = 0; j < 8; ++j) {
+                        const uint2 r = a.cells[o * 8u + (uint32_t)j];
+                        if (r.x != 0xffffffffu) r1 = max(r1, r.y + 1u);
+                    }
+                }
+                S.end = r1;
+                S.next = 0u;
+                S.box[0] = S.box[1] = S.box[2] = 0x7fffffff;
+                S.box[3] = S.box[4] = S.box[5] = -0x7fffffff;
+                S.defer_all = 0;
+                S.hmax_bits = 0;
             }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                b[k] = __reduce_min_sync(0xffffffffu, b[k]);
-                b[k + 3] = __reduce_max_sync(0xffffffffu, b[k + 3]);
-            }
-            if (lane == 0) {
-#pragma unroll
+            __syncthreads();
+            const uint32_t start = r0, end = S.end;
+            {
+                int b[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, -0x7fffffff, -0x7fffffff, -0x7fffffff};
+                for (uint32_t p = start + tid; p < end; p += kTileThreads) {
+                    if (!a.active[a.cidx[p]]) continue;
+                    const float4 A = a.sA[p];
+                    CellBox cb;
+                    if (!accel_box(A.x, A.y, A.z, A.w, cb)) continue;
+                    b[0] = min(b[0], cb.lo0);
+                    b[1] = min(b[1], cb.lo1);
+                    b[2] = min(b[2], cb.lo2);
+                    b[3] = max(b[3], cb.hi0);
+                    b[4] = max(b[4], cb.hi1);
+                    b[5] = max(b[5], cb.hi2);
+                }
+    #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    atomicMin(&S.box[k], b[k]);
-                    atomicMax(&S.box[k + 3], b[k + 3]);
+                    b[k] = __reduce_min_sync(0xffffffffu, b[k]);
+                    b[k + 3] = __reduce_max_sync(0xffffffffu, b[k + 3]);
+                }
+                if (lane == 0) {
+    #pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        atomicMin(&S.box[k], b[k]);
+                        atomicMax(&S.box[k + 3], b[k + 3]);
+                    }
                 }
             }
-        }
-        __syncthreads();
-        const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
-        const bool any = lo0 <= S.box[3];
-        const int nx = any ? S.box[3] - lo0 + 1 : 0, ny = any ? S.box[4] - lo1 + 1 : 0,
-                  nz = any ? S.box[5] - lo2 + 1 : 0;
-        int ncell = 0;
-        if (any) {
-            if (nx * ny * nz > kTileCellsMax) {
-                if (tid == 0) S.defer_all = 1;
-            } else {
-                ncell = nx * ny * nz;
-            }
-        }
-        uint32_t c_cnt[kTileCellsPerThread];
-        uint32_t tsum = 0u;
-#pragma unroll
-        for (int k = 0; k < kTileCellsPerThread; ++k) {
-            const int c = kTileCellsPerThread * tid + k;
-            c_cnt[k] = 0u;
-            if (c < ncell) {
-                const int ix = c / (ny * nz), rem = c - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
-                const uint2 r = __ldg(a.cells + cell_index_of(lo0 + ix, lo1 + iy, lo2 + iz));
-                if (r.x != 0xffffffffu) {
-                    c_cnt[k] = r.y - r.x + 1u;
-                    S.first[c] = r.x;
+            __syncthreads();
+            const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
+            const bool any = lo0 <= S.box[3];
+            const int nx = any ? S.box[3] - lo0 + 1 : 0, ny = any ? S.box[4] - lo1 + 1 : 0,
+                      nz = any ? S.box[5] - lo2 + 1 : 0;
+            int ncell = 0;
+            if (any) {
+                if (nx * ny * nz > kTileCellsMax) {
+                    if (tid == 0) S.defer_all = 1;
+                } else {
+                    ncell = nx * ny * nz;
                 }
             }
-            tsum += c_cnt[k];
-        }
-        uint32_t inc = tsum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        if (lane == 31) S.wsum[tid >> 5] = inc;
-        __syncthreads();
-        uint32_t wbase = 0u;
-        for (int w = 0; w < (tid >> 5); ++w) wbase += S.wsum[w];
-        uint32_t run = wbase + inc - tsum;
-#pragma unroll
-        for (int k = 0; k < kTileCellsPerThread; ++k) {
-            const int c = kTileCellsPerThread * tid + k;
-            if (c < ncell) S.off[c] = run;
-            run += c_cnt[k];
-        }
-        if (tid == kTileThreads - 1) {
-            S.off[ncell] = run;
-            if (run > (uint32_t)kTileAccStage) S.defer_all = 1;
-        }
-        __syncthreads();
-        float hmax = 0.f;
-        if (!S.defer_all) {
-            const uint32_t total = S.off[ncell];
-            for (uint32_t s = tid; s < total; s += kTileThreads) {
-                int lo = 0, hi = ncell - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (S.off[mid] <= s) lo = mid;
-                    else hi = mid - 1;
+            uint32_t c_cnt[kTileCellsPerThread];
+            uint32_t tsum = 0u;
+    #pragma unroll
+            for (int k = 0; k < kTileCellsPerThread; ++k) {
+                const int c = kTileCellsPerThread * tid + k;
+                c_cnt[k] = 0u;
+                if (c < ncell) {
+                    const int ix = c / (ny * nz), rem = c - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
+                    const uint2 r = __ldg(a.cells + cell_index_of(lo0 + ix, lo1 + iy, lo2 + iz));
+                    if (r.x != 0xffffffffu) {
+                        c_cnt[k] = r.y - r.x + 1u;
+                        S.first[c] = r.x;
+                    }
                 }
-                const uint32_t gi = S.first[lo] + (s - S.off[lo]);
-                const float4 q = __ldg(a.sA + gi);
-                S.pos[s] = q;
-                S.gidx[s] = gi;
-                const int ix = lo / (ny * nz), rem = lo - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
-                S.scell[s] = (uint32_t)ix | ((uint32_t)iy << 10) | ((uint32_t)iz << 20);
-                hmax = fmaxf(hmax, q.w);
+                tsum += c_cnt[k];
             }
+            uint32_t inc = tsum;
+    #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            if (lane == 31) S.wsum[tid >> 5] = inc;
+            __syncthreads();
+            uint32_t wbase = 0u;
+            for (int w = 0; w < (tid >> 5); ++w) wbase += S.wsum[w];
+            uint32_t run = wbase + inc - tsum;
+    #pragma unroll
+            for (int k = 0; k < kTileCellsPerThread; ++k) {
+                const int c = kTileCellsPerThread * tid + k;
+                if (c < ncell) S.off[c] = run;
+                run += c_cnt[k];
+            }
+            if (tid == kTileThreads - 1) {
+                S.off[ncell] = run;
+                if (run > (uint32_t)kTileAccStage) S.defer_all = 1;
+            }
+            __syncthreads();
+            if (S.defer_all && whole && splittable) {
+                whole = false;
+                continue;
+            }
+            float hmax = 0.f;
+            if (!S.defer_all) {
+                const uint32_t total = S.off[ncell];
+                for (uint32_t s = tid; s < total; s += kTileThreads) {
+                    int lo = 0, hi = ncell - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (S.off[mid] <= s) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    const uint32_t gi = S.first[lo] + (s - S.off[lo]);
+                    const float4 q = __ldg(a.sA + gi);
+                    S.pos[s] = q;
+                    S.gidx[s] = gi;
+                    const int ix = lo / (ny * nz), rem = lo - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
+                    S.scell[s] = (uint32_t)ix | ((uint32_t)iy << 10) | ((uint32_t)iz << 20);
+                    hmax = fmaxf(hmax, q.w);
+                }
+            }
+            {
+                float v = hmax;
+    #pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+                if (lane == 0 && v > 0.f) atomicMax(&S.hmax_bits, __float_as_int(v));
+            }
+            __syncthreads();
+            int wmin = 0x7fffffff;
+            for (;;) {
+                uint32_t j = 0u;
+                if (lane == 0) j = atomicAdd(&S.next, (uint32_t)kTileGpw);
+                j = __shfl_sync(0xffffffffu, j, 0);
+                if (start + j >= end) break;
+                wmin = min(wmin, accel_tile_warp<KAHAN>(a, S, start + j, end, lane, tid >> 5, deferred, ctr + 2));
+            }
+            if (lane == 0 && wmin != 0x7fffffff) atomicMin(&S.dtmin, wmin);
+            r0 = end;
         }
-        {
-            float v = hmax;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-            if (lane == 0 && v > 0.f) atomicMax(&S.hmax_bits, __float_as_int(v));
-        }
-        __syncthreads();
-        int wmin = 0x7fffffff;
-        for (;;) {
-            uint32_t j = 0u;
-            if (lane == 0) j = atomicAdd(&S.next, 4u);
-            j = __shfl_sync(0xffffffffu, j, 0);
-            if (start + j >= end) break;
-            wmin = min(wmin, accel_tile_warp<KAHAN>(a, S, start + j, end, lane, tid >> 5, deferred, ctr + 2));
-        }
-        if (lane == 0 && wmin != 0x7fffffff) atomicMin(&S.dtmin, wmin);
     }
     if (tid == 0 && S.dtmin != 0x7fffffff) atomicMin(a.globals + 1, S.dtmin);
 }
@@ -1889,6 +1969,7 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     DensityArgs a;
     a.n = n;
     a.cidx = cidx;
+    a.skey = ctx->cell_sort.keys[ctx->cell_final];
     a.cells = ctx->cell_range;
     a.sp4 = ctx->sp4;
     a.sv4 = ctx->sv4;
@@ -1947,6 +2028,7 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     AccelArgs a;
     a.n = n;
     a.cidx = ctx->cell_sort.vals[ctx->cell_final];
+    a.skey = ctx->cell_sort.keys[ctx->cell_final];
     a.cells = ctx->cell_range;
     a.sA = ctx->sA;
     a.sB = ctx->sB;

@@ -117,6 +117,11 @@ def main(ref_root: str | None = None):
     st = O.OracleState(ic, ef, ee, kind="ref")
     out = {f"ic_{k}": np.asarray(v) for k, v in ic.items() if isinstance(v, np.ndarray)}
     out["file_sha256"] = file_digest
+    # Compute::drawSnapshot of the initial state, the reference's kernel
+    # (render.metal:49-66); stored as the set pixels
+    img = O.draw_snapshot_ref(ic["pos"], ic["material"]).reshape(-1)
+    out["snapshot_pixel"] = np.nonzero(img)[0].astype(np.int32)
+    out["snapshot_material"] = img[out["snapshot_pixel"]]
     for s in range(2):
         t = O.tree_reference(st.pos, 4, kind="ref")
         st.set_tree(t)

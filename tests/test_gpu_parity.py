@@ -262,21 +262,22 @@ def test_step_all_graph_equals_eager(cuda, pkg):
             assert np.array_equal(a.download(f).view(np.uint8), b.download(f).view(np.uint8)), f
 
 
-def test_snapshot_splat(cuda, pkg):
+def test_snapshot_splat(cuda, pkg, O):
+    """Compute::drawSnapshot (render.metal:49-66): the GPU splat equals the
+    oracle's restatement (pinned to the reference's kernel in
+    test_oracle_golden) on a synthetic impact, and the reference's own splat
+    of its demo input (golden fixture)."""
     ic = pkg.ic.make_impact(4096, 1024, seed=0)
     with pkg.Compute(ic) as c:
         img = c.drawSnapshot()
-    # render.metal:49-66 on the host
-    p = ic["pos"].astype(np.float32)
-    R_E = np.float32(6.3710)
-    s = np.float32(1024) / (np.float32(20) * R_E)
-    ux = (p[:, 0] - np.float32(250)) * s
-    uy = (p[:, 1] - np.float32(250)) * s
-    ok = (ux >= 0) & (uy >= 0) & (ux < 1024) & (uy < 1024)
-    px = ux[ok].astype(np.int64) + (1023 - uy[ok].astype(np.int64)) * 1024
-    want = np.zeros(1024 * 1024, np.int64)
-    np.maximum.at(want, px, ic["material"][ok].astype(np.int64))
-    assert np.array_equal(img.reshape(-1), want.astype(np.int32))
+    assert np.array_equal(img.reshape(1024, 1024), O.draw_snapshot(ic["pos"], ic["material"]))
+    g = golden("demo_impact_n40.npz")
+    ic = {k[3:]: v for k, v in g.items() if k.startswith("ic_")}
+    want = np.zeros(1024 * 1024, np.int32)
+    want[g["snapshot_pixel"]] = g["snapshot_material"]
+    with pkg.Compute(ic, max_children_in_leaf=4) as c:
+        img = c.drawSnapshot()
+    assert np.array_equal(img.reshape(-1), want)
 
 
 STATE = ("pos", "vel", "u", "h", "rho", "pressure", "grad_term", "sound_speed", "balsara", "grav_norm", "active",

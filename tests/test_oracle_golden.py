@@ -122,3 +122,22 @@ def test_config0_ten_steps_match_reference_digests(O, eos_grids, pkg):
                 assert np.array_equal(d, want[f"s{s}_{p}_{f}"]), f"step {s} {p} {f}"
     for f in ("pos", "vel", "u", "h", "rho"):
         assert np.array_equal(bits(getattr(st, f)), bits(g[f"final_{f}"])), f
+
+
+def test_snapshot_splat_matches_reference_kernel(O, pkg):
+    """The oracle's splat equals the reference's drawToSnapshot
+    (render.metal:49-66, built into oracle/_ref when the reference tree is
+    present) and the reference's splat of its demo input (golden fixture)."""
+    import os
+    g = golden("demo_impact_n40.npz")
+    want = np.zeros(1024 * 1024, np.int32)
+    want[g["snapshot_pixel"]] = g["snapshot_material"]
+    assert np.array_equal(O.draw_snapshot(g["ic_pos"], g["ic_material"]).reshape(-1), want)
+    if not os.path.exists(O.REF_PATH):
+        pytest.skip("reference build (oracle/_ref) not present")
+    ic = pkg.ic.make_impact(4096, 1024, seed=0)
+    assert np.array_equal(O.draw_snapshot(ic["pos"], ic["material"]), O.draw_snapshot_ref(ic["pos"], ic["material"]))
+    # splats on the edges: x exactly 250 Mm and just inside the far side
+    p = np.array([[250.0, 250.0, 0.0], [250.0 + 127.42 * 0.999, 300.0, 0.0], [249.99, 300.0, 0.0]], np.float32)
+    m = np.array([400, 402, 400], np.int32)
+    assert np.array_equal(O.draw_snapshot(p, m), O.draw_snapshot_ref(p, m))
