@@ -160,6 +160,14 @@ sph_status sph_step(sph_ctx *ctx, void *stream);         /* Compute::stepPass (:
 #define SPH_PRECISION_REFERENCE 0 /* float positions drifted in float, as the reference (step.metal:45) */
 #define SPH_PRECISION_MIXED     1 /* FP64 master positions and global time (float working copies), Kahan-
                                      compensated acceleration, du/dt and dh/dt sums */
+#define SPH_TIMESTEP_GLOBAL     0 /* the reference's active test as shipped, globalTime <= nextActiveTime
+                                     (P2M.metal:31): every particle is active every step */
+#define SPH_TIMESTEP_INDIVIDUAL 1 /* README.md:60-64 as described: a particle is active once the global time
+                                     reaches its next active time; a leaf with an active particle, and a branch
+                                     of leaves with an active leaf, activate all their particles; inactive
+                                     particles are only integrated (no gravity, neighbour or acceleration
+                                     work); the global step never passes an inactive particle's next
+                                     active time */
 #define SPH_HSEED_PLAIN   0 /* the iteration starts from the particle's own h (density.metal:73-74) */
 #define SPH_HSEED_LEARNED 1 /* it starts from the learned seed (sph_hseed_train), with fallback */
 typedef struct {
@@ -170,6 +178,7 @@ typedef struct {
     int32_t h_seed;    /* SPH_HSEED_* */
     int32_t precision; /* SPH_PRECISION_* */
     float h_tolerance; /* convergence test of the h iteration, |dh| / h <= tol; 0 = DENSITY_ETA (0.005) */
+    int32_t timestep;  /* SPH_TIMESTEP_* */
 } sph_form;
 void sph_form_default(sph_form *f); /* reference form, theta 0.5 */
 /* Select the form for the following passes (drops a captured step graph).

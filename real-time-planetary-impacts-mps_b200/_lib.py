@@ -73,7 +73,7 @@ class SphIC(C.Structure):
 
 class SphForm(C.Structure):
     _fields_ = [("gravity", C.c_int32), ("theta", C.c_float), ("h_seed", C.c_int32), ("precision", C.c_int32),
-                ("h_tolerance", C.c_float)]
+                ("h_tolerance", C.c_float), ("timestep", C.c_int32)]
 
 
 class SphEnsembleTuning(C.Structure):

@@ -81,7 +81,7 @@ def _ic_struct(ic: dict):
 
 
 def _form(lib, gravity: str = "reference", theta: float = 0.5, precision: str = "reference",
-          h_seed: str = "plain", h_tolerance: float = 0.0) -> "_lib.SphForm":
+          h_seed: str = "plain", h_tolerance: float = 0.0, timestep: str = "global") -> "_lib.SphForm":
     f = _lib.SphForm()
     lib.sph_form_default(C.byref(f))
     f.gravity = _lib.SPH_GRAVITY_THETA if gravity == "theta" else _lib.SPH_GRAVITY_REFERENCE
@@ -89,6 +89,9 @@ def _form(lib, gravity: str = "reference", theta: float = 0.5, precision: str = 
     f.precision = _lib.SPH_PRECISION_MIXED if precision == "mixed" else _lib.SPH_PRECISION_REFERENCE
     f.h_seed = _lib.SPH_HSEED_LEARNED if h_seed == "learned" else _lib.SPH_HSEED_PLAIN
     f.h_tolerance = float(h_tolerance)
+    if timestep not in ("global", "individual"):
+        raise ValueError(f"timestep must be 'global' or 'individual', not {timestep!r}")
+    f.timestep = 1 if timestep == "individual" else 0
     return f
 
 
@@ -222,14 +225,17 @@ class Compute:
 
     # ---- numerical forms (no reference counterpart) --------------------
     def set_form(self, gravity: str = "reference", theta: float = 0.5, precision: str = "reference",
-                 h_seed: str = "plain", h_tolerance: float = 0.0):
+                 h_seed: str = "plain", h_tolerance: float = 0.0, timestep: str = "global"):
         """Select the numerical form: gravity "reference" (the reference's
         logic) or "theta" (opening-angle group walk with exact near field);
         precision "reference" (float positions) or "mixed" (FP64 master
         positions and time, Kahan-compensated sums); h_seed "plain" or
         "learned" (the trained MLP starts the density iteration);
-        h_tolerance of the density iteration (0 = the reference's 0.005)."""
-        f = _form(self._lib, gravity, theta, precision, h_seed, h_tolerance)
+        h_tolerance of the density iteration (0 = the reference's 0.005);
+        timestep "global" (the reference's active test as shipped: every
+        particle every step) or "individual" (particles active only when their
+        next active time is reached, README.md:60-64)."""
+        f = _form(self._lib, gravity, theta, precision, h_seed, h_tolerance, timestep)
         self._check(self._lib.sph_set_form(self._h, C.byref(f)), "sph_set_form")
 
     def get_form(self) -> dict:
@@ -237,7 +243,8 @@ class Compute:
         self._check(self._lib.sph_get_form(self._h, C.byref(f)), "sph_get_form")
         return dict(gravity="theta" if f.gravity == _lib.SPH_GRAVITY_THETA else "reference", theta=f.theta,
                     precision="mixed" if f.precision == _lib.SPH_PRECISION_MIXED else "reference",
-                    h_seed="learned" if f.h_seed == _lib.SPH_HSEED_LEARNED else "plain", h_tolerance=f.h_tolerance)
+                    h_seed="learned" if f.h_seed == _lib.SPH_HSEED_LEARNED else "plain", h_tolerance=f.h_tolerance,
+                    timestep="individual" if f.timestep == 1 else "global")
 
     # ---- learned smoothing-length seed (no reference counterpart) ------
     def hseed_capture(self, on: bool = True):
@@ -417,7 +424,7 @@ class Compute:
         out = {f: self.download(f) for f in self.CHECKPOINT_FIELDS}
         form = self.get_form()
         out["form"] = np.array([form["gravity"], str(form["theta"]), form["precision"], form["h_seed"],
-                                str(form["h_tolerance"])])
+                                str(form["h_tolerance"]), form["timestep"]])
         out["tree_source"] = np.array([self.tree_source])
         out["params"] = np.array(self._params_tuple, np.int64)
         if form["precision"] == "mixed":
@@ -439,12 +446,12 @@ class Compute:
         c = cls(ic, max_children_in_leaf=leaf, max_tree_depth=depth, max_unchecked_pointers=unchecked,
                 aneos_resolution=res, tree_source=str(ck["tree_source"][0]), forsterite_table=forsterite_table,
                 fe85si15_table=fe85si15_table, parity=parity)
-        g, th, prec, seed, tol = (str(v) for v in ck["form"])
+        g, th, prec, seed, tol, ts = (str(v) for v in ck["form"])
         if "hseed_params" in ck:
             c.hseed_params(ck["hseed_params"])
             c.hseed_norm(ck["hseed_norm"])
             c.upload("neighbours", ck["neighbours"])
-        c.set_form(gravity=g, theta=float(th), precision=prec, h_seed=seed, h_tolerance=float(tol))
+        c.set_form(gravity=g, theta=float(th), precision=prec, h_seed=seed, h_tolerance=float(tol), timestep=ts)
         for f in cls.CHECKPOINT_FIELDS:
             if f not in ic:
                 c.upload(f, ck[f])

@@ -888,6 +888,7 @@ void sph_form_default(sph_form *f) {
     f->h_seed = SPH_HSEED_PLAIN;
     f->precision = SPH_PRECISION_REFERENCE;
     f->h_tolerance = 0.f;
+    f->timestep = SPH_TIMESTEP_GLOBAL;
 }
 
 sph_status sph_set_form(sph_ctx *ctx, const sph_form *f) {
@@ -910,6 +911,10 @@ sph_status sph_set_form(sph_ctx *ctx, const sph_form *f) {
     }
     if (!(f->h_tolerance >= 0.f && f->h_tolerance < 1.f)) {
         set_error("sph_set_form: h_tolerance = %g is outside [0, 1)", (double)f->h_tolerance);
+        return SPH_ERR_INVALID_ARG;
+    }
+    if (f->timestep != SPH_TIMESTEP_GLOBAL && f->timestep != SPH_TIMESTEP_INDIVIDUAL) {
+        set_error("sph_set_form: timestep = %d is not a SPH_TIMESTEP_* value", (int)f->timestep);
         return SPH_ERR_INVALID_ARG;
     }
     if (f->precision != SPH_PRECISION_REFERENCE && f->precision != SPH_PRECISION_MIXED) {

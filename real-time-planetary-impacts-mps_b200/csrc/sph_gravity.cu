@@ -88,6 +88,7 @@ struct UpArgs {
     uint8_t *active;
     const int32_t *nat;
     const int32_t *globals;
+    int individual;  // SPH_TIMESTEP_INDIVIDUAL: active once the time reaches nextActiveTime
 };
 
 // P2M.metal:12-107
@@ -103,7 +104,9 @@ __device__ void p2m(const UpArgs &a, int tp, int dp) {
     for (int i = s; i < e; ++i) {
         const int p = T[i];
         const float4 q = a.pos4[p];
-        const bool ia = gt <= a.nat[p];  // reference quirk: active while time <= next
+        // the reference's test as shipped is time <= next (every particle
+        // active every step); the individual form uses README.md:62's
+        const bool ia = a.individual ? gt >= a.nat[p] : gt <= a.nat[p];
         if (!act && ia) act = true;
         mxx = fmax_ref(mxx, q.x);
         mxy = fmax_ref(mxy, q.y);
@@ -586,6 +589,7 @@ sph_status launch_gravity(sph_ctx *ctx, cudaStream_t st) {
     u.active = ctx->active;
     u.nat = ctx->nat;
     u.globals = ctx->globals;
+    u.individual = ctx->form.timestep == SPH_TIMESTEP_INDIVIDUAL;
     for (int l = L - 1; l >= 0; --l) {
         int64_t bound = tr.level_count_host[l];
         int blocks = (int)((bound + 127) / 128);

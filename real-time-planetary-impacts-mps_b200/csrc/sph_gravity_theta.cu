@@ -51,6 +51,9 @@ struct ThetaUpArgs {
     float4 *poles;
     const float4 *pos4;
     uint8_t *active;
+    const int32_t *nat;
+    const int32_t *globals;
+    int individual;  // SPH_TIMESTEP_INDIVIDUAL: activity from the next active times, synced per leaf
 };
 
 __device__ void p2m_theta(const ThetaUpArgs &a, int tp, int dp) {
@@ -61,10 +64,18 @@ __device__ void p2m_theta(const ThetaUpArgs &a, int tp, int dp) {
     const float4 x0 = a.pos4[T[s]];
     float m = 0.f, sx = 0.f, sy = 0.f, sz = 0.f;
     float mnx = x0.x, mny = x0.y, mnz = x0.z, mxx = x0.x, mxy = x0.y, mxz = x0.z;
+    // individual timesteps: the leaf is active when one of its particles is
+    // due, and then all of them are (README.md:62-64); otherwise all are
+    bool act = true;
+    if (a.individual) {
+        const int gt = a.globals[0];
+        act = false;
+        for (int i = 0; i < np && !act; ++i) act = gt >= a.nat[T[s + i]];
+    }
     for (int i = 0; i < np; ++i) {
         const int p = T[s + i];
         const float4 q = a.pos4[p];
-        a.active[p] = 1;
+        a.active[p] = act ? 1 : 0;
         m += q.w;
         sx += q.w * (q.x - x0.x);
         sy += q.w * (q.y - x0.y);
@@ -94,7 +105,7 @@ __device__ void p2m_theta(const ThetaUpArgs &a, int tp, int dp) {
     pr[1] = make_float4(m, qxx, qxy, qxz);
     pr[2] = make_float4(qyy, qyz, qzz, 0.f);
     pr[3] = make_float4(mnx, mny, mnz, 0.f);
-    pr[4] = make_float4(mxx, mxy, mxz, 1.f);
+    pr[4] = make_float4(mxx, mxy, mxz, act ? 1.f : 0.f);
     pr[5] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
@@ -143,13 +154,35 @@ __device__ void m2m_theta(const ThetaUpArgs &a, int tp, int dp) {
         qyz += q2.y + mc * ry * rz;
         qzz += q2.z + mc * rz * rz;
     }
+    // individual timesteps: a branch is active when a child is; a branch
+    // whose children are all leaves activates every leaf and particle under
+    // it when one leaf is active (README.md:64)
+    bool act = true;
+    if (a.individual) {
+        act = false;
+        bool all_leaves = true;
+        for (int k = 0; k < 8; ++k) {
+            const int c = T[tp + 2 + k];
+            if (c == -1) continue;
+            if (a.poles[(size_t)T[c + 1] * kPoleQ + 4].w != 0.f) act = true;
+            if (T[c] == 0) all_leaves = false;
+        }
+        if (act && all_leaves) {
+            for (int k = 0; k < 8; ++k) {
+                const int c = T[tp + 2 + k];
+                if (c == -1) continue;
+                a.poles[(size_t)T[c + 1] * kPoleQ + 4].w = 1.f;
+                for (int j = 0; j < T[c]; ++j) a.active[T[c + 2 + j]] = 1;
+            }
+        }
+    }
     const float cx = c0f.x + ox, cy = c0f.y + oy, cz = c0f.z + oz;
     float4 *pr = a.poles + (size_t)dp * kPoleQ;
     pr[0] = make_float4(cx, cy, cz, corner_radius(cx, cy, cz, mnx, mny, mnz, mxx, mxy, mxz));
     pr[1] = make_float4(m, qxx, qxy, qxz);
     pr[2] = make_float4(qyy, qyz, qzz, 0.f);
     pr[3] = make_float4(mnx, mny, mnz, 0.f);
-    pr[4] = make_float4(mxx, mxy, mxz, 1.f);
+    pr[4] = make_float4(mxx, mxy, mxz, act ? 1.f : 0.f);
     pr[5] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
@@ -239,6 +272,7 @@ struct WalkArgs {
     int32_t *queues;
     uint32_t *counter;
     uint32_t *health;
+    const uint8_t *active;  // individual timesteps: only active particles are walked for and written
 };
 
 // Acceleration (and potential) of the staged nodes at x, per unit G.
@@ -317,6 +351,10 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(WalkArgs a) {
         if (g >= a.ngroups) break;
         const int i = g * 32 + lane;
         const bool valid = i < a.n;
+        // individual timesteps: only active particles get gravity, and a
+        // group without one is skipped (the down-pass culling of README.md:64)
+        const bool act = valid && (!a.active || a.active[a.order[i]]);
+        if (!__any_sync(full, act)) continue;
         const float4 xi = a.kp4[valid ? i : g * 32];
         float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f, cax = 0.f, cay = 0.f, caz = 0.f, cph = 0.f;
         int ncell = 0, nleaf = 0;
@@ -484,7 +522,7 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(WalkArgs a) {
                 walk();
             }
         }
-        if (valid) {
+        if (act) {
             const uint32_t id = a.order[i];
             if (ACC) {
                 const float4 old = a.acc4[id];
@@ -575,6 +613,11 @@ static sph_status theta_pass(sph_ctx *ctx, float theta, bool acc, cudaStream_t s
     u.poles = tr.poles;
     u.pos4 = ctx->pos4;
     u.active = ctx->active;
+    u.nat = ctx->nat;
+    u.globals = ctx->globals;
+    // activity follows the next active times only when the accelerations are
+    // computed (the potential for the diagnostics covers every particle)
+    u.individual = acc && ctx->form.timestep == SPH_TIMESTEP_INDIVIDUAL;
     for (int l = L - 1; l >= 0; --l) {
         int64_t bound = tr.level_count_host[l];
         int blocks = (int)((bound + 127) / 128);
@@ -626,6 +669,7 @@ static sph_status theta_pass(sph_ctx *ctx, float theta, bool acc, cudaStream_t s
     w.queues = tb.walk_queues;
     w.counter = tb.walk_counter;
     w.health = ctx->health;
+    w.active = u.individual ? ctx->active : nullptr;
     if (acc)
         k_walk<true><<<blocks, 32 * kWalkWarps, 0, st>>>(w);
     else

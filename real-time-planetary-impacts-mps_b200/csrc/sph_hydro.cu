@@ -1178,7 +1178,16 @@ struct AccelArgs {
     int32_t *nat;
     const uint8_t *active;
     int32_t *globals;
+    int individual;  // SPH_TIMESTEP_INDIVIDUAL: inactive particles bound the global step
 };
+
+// The ticks an inactive particle allows the global step: INT_MAX with the
+// reference's test (all particles active anyway); with individual timesteps
+// the time left to its next active time, so no step passes it.
+__device__ __forceinline__ int inactive_ticks(const AccelArgs &a, uint32_t ind) {
+    if (!a.individual) return 0x7fffffff;
+    return max(a.nat[ind] - a.globals[0], 1);
+}
 
 // The particle's own terms of accelerations.metal:60-141.
 struct AccelI {
@@ -1302,7 +1311,7 @@ template <int L, bool KAHAN>
 __device__ __forceinline__ int accel_particle(const AccelArgs &a, int index, int sub, unsigned gm, int gbase,
                                               uint32_t *w_off, uint32_t *w_start, uint32_t *list) {
     const uint32_t ind = a.cidx[index];
-    if (!a.active[ind]) return 0x7fffffff;
+    if (!a.active[ind]) return inactive_ticks(a, ind);
     const AccelI I = accel_i(a.sA[index], a.sB[index], a.sC[index]);
     AccelSum S;
     const float4 *sA = a.sA, *sB = a.sB, *sC = a.sC;
@@ -1438,9 +1447,11 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
     const uint32_t p = p0 + (uint32_t)g;
     bool live = p < end;
     uint32_t ind = 0u;
+    int idt_inactive = 0x7fffffff;
     if (live) {
         ind = a.cidx[p];
         live = a.active[ind] != 0;
+        if (!live) idt_inactive = inactive_ticks(a, ind);
     }
     float4 A = make_float4(0.f, 0.f, 0.f, 1.f), Bv = A, Cv = A;
     if (live) {
@@ -1478,7 +1489,7 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
               u2 = __reduce_min_sync(kFull, b.lo2);
     const int v0 = __reduce_max_sync(kFull, b.hi0), v1 = __reduce_max_sync(kFull, b.hi1),
               v2 = __reduce_max_sync(kFull, b.hi2);
-    if (u0 > v0) return 0x7fffffff;  // no active particle takes the tile path
+    if (u0 > v0) return __reduce_min_sync(kFull, idt_inactive);  // no active particle takes the tile path
     __syncwarp();
     // every accepted pair lies within 2 max(h_i, largest staged h) of the particle
     const float hm = fmaxf(I.hi, __int_as_float(S.hmax_bits));
@@ -1599,7 +1610,7 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
         }
     }
     accel_reduce<L, KAHAN>(Sm, kFull);
-    int idt = 0x7fffffff;
+    int idt = idt_inactive;
     if (live) {
         idt = accel_ticks(I, Sm.vsig);
         if (sub == 0) accel_store(a, ind, Sm, idt);
@@ -2039,6 +2050,7 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     a.nat = ctx->nat;
     a.active = ctx->active;
     a.globals = ctx->globals;
+    a.individual = ctx->form.timestep == SPH_TIMESTEP_INDIVIDUAL;
     constexpr int parts = parts_per_block<kLanesPerParticle>();
     const size_t smem = list_smem_opt_in();
     const bool kahan = ctx->form.precision == SPH_PRECISION_MIXED;

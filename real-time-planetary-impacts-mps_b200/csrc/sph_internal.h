@@ -140,7 +140,7 @@ struct sph_ctx {
     double4 *pos64 = nullptr;
     double *dglob = nullptr;
     double *diag = nullptr;  // diagnostics: block partials, then the totals
-    sph_form form{SPH_GRAVITY_REFERENCE, 0.5f, SPH_HSEED_PLAIN, SPH_PRECISION_REFERENCE, 0.f};
+    sph_form form{SPH_GRAVITY_REFERENCE, 0.5f, SPH_HSEED_PLAIN, SPH_PRECISION_REFERENCE, 0.f, SPH_TIMESTEP_GLOBAL};
     int32_t *mat = nullptr, *nat = nullptr;
     uint8_t *active = nullptr;
     int32_t *globals = nullptr;
