@@ -171,11 +171,20 @@ def host_cores() -> dict:
     return {"logical": logical, "physical": physical}
 
 
+def set_omp_threads(n: int):
+    """Threads of the OpenMP runtime the host reference library runs on."""
+    try:
+        ctypes.CDLL("libgomp.so.1").omp_set_num_threads(int(n))
+    except OSError:
+        pass
+    os.environ["OMP_NUM_THREADS"] = str(n)
+
+
 def cpu_reference(ic: dict, steps: int, warmup: int, budget_s: float | None = None, threads: int | None = None) -> dict:
     """The reference's kernels on the host cores (oracle/_ref when built, else
     the oracle restatement), full N, reference CPU octree rebuilt every step."""
     if threads:
-        os.environ["OMP_NUM_THREADS"] = str(threads)
+        set_omp_threads(threads)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O  # noqa: E402 -- CPU-baseline leg only
     eos_mod = importlib.import_module("real-time-planetary-impacts-mps_b200.eos_tables")
@@ -443,13 +452,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="particle count relative to 1e6 (diagnostics)")
     ap.add_argument("--theta", type=float, default=0.6, help="opening angle of the chosen form's gravity")
-    ap.add_argument("--train-iters", type=int, default=150, help="Adam steps after each warm-up step")
+    ap.add_argument("--train-iters", type=int, default=600, help="Adam steps after each warm-up step")
     ap.add_argument("--drift-steps", type=int, default=100,
                     help="steps of the energy-drift comparison (the 1000-step comparison runs at config 0 in the tests)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="time the batched ensemble of this many impacts instead of the N=1e6 impact")
     ap.add_argument("--ensemble-seed", type=int, default=0)
     ap.add_argument("--autotune", action="store_true", help="ensemble: tune tiles and leaf capacity per instance")
+    ap.add_argument("--single-thread-baseline", action="store_true",
+                    help="also time the CPU reference on one thread (about two minutes at N=1e6)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -627,9 +638,15 @@ def main():
         line.update(extra)
         if not args.no_cpu_baseline and world == 1:
             log("cpu baseline ...")
-            cb = cpu_reference(ic, steps=10, warmup=1, budget_s=20.0)
+            hc = host_cores()
+            cb = cpu_reference(ic, steps=10, warmup=1, budget_s=20.0, threads=hc["logical"])
             log(f"cpu baseline: {cb['value']:.3e} particle-steps/s on {cb['cores']} threads")
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "physical_cores")}
+            if args.single_thread_baseline:
+                one = cpu_reference(ic, steps=1, warmup=1, threads=1)
+                log(f"cpu baseline, one thread: {one['value']:.3e} particle-steps/s")
+                line["cpu_baseline"]["single_thread"] = {"value": one["value"], "cores": 1, "sample": one["sample"]}
+                set_omp_threads(hc["logical"])
         print(json.dumps(line), flush=True)
     cp.close()
     cc.close()

@@ -294,6 +294,14 @@ sph_status sph_sort_cells_noalloc_health(void *stream, uint32_t *word);
  * returns SPH_ERR_TIMEOUT).  The GPU stays usable; clear the word afterwards
  * (sph_clear_health, or the next sph_sort_cells_noalloc call). */
 sph_status sph_selftest_lookback_timeout(sph_ctx *ctx, int32_t spin_limit, void *stream);
+/* Self-test of the GPU tree build's capacity check (no counterpart in the
+ * reference): one tree build runs with its storage bound lowered to 16 ints,
+ * so the layout kernels find the tree too large, skip the writes that would
+ * not fit and raise SPH_HEALTH_TREE_CAPACITY (sph_synchronize then returns
+ * SPH_ERR_DEVICE_HEALTH).  The storage itself is untouched beyond the bound;
+ * the tree is marked stale, the next tree build (sph_update_tree, sph_step)
+ * makes a whole one.  SPH_TREE_GPU contexts only. */
+sph_status sph_selftest_tree_capacity(sph_ctx *ctx, void *stream);
 
 /* n_steps x (tree, sort, gravity, density, acceleration, step), replayed from
  * a CUDA graph captured on first use (Headless::step without the snapshot). */

@@ -183,6 +183,7 @@ def load(parity: bool = False) -> C.CDLL:
         "sph_sort_cells_noalloc": (st, [vp, C.c_int32, vp, vp, vp]),
         "sph_sort_cells_noalloc_health": (st, [vp, C.POINTER(C.c_uint32)]),
         "sph_selftest_lookback_timeout": (st, [vp, C.c_int32, vp]),
+        "sph_selftest_tree_capacity": (st, [vp, vp]),
         "sph_upload_async": (st, [vp, C.c_int, vp, C.c_size_t, vp]),
         "sph_download_async": (st, [vp, C.c_int, vp, C.c_size_t, vp]),
         "sph_form_default": (None, [C.POINTER(SphForm)]),

@@ -633,26 +633,28 @@ __device__ __forceinline__ float tile_start_h(const DensityArgs &a, uint32_t ind
     return h_plain;
 }
 
-// Tiles: at the first sorted particle of every occupied 64-cell block, the
-// block's octet ranges (from its 64 cell ranges); the block is one tile when it
-// holds at most block_max particles, else each 16-cell quarter is one when it
-// holds at most half_max, else each octet is.  (first, one past last)
-// per tile, in ticket order.  ctr[0] counts tiles; ctr[1] is the CTAs' tile
-// ticket, ctr[2] the deferred count.
+// Tiles: at the first sorted particle of every occupied 128-cell block (the
+// cells whose keys differ in the low seven bits, 4 x 4 x 8), the block's
+// octet ranges (from its 128 cell ranges); the block is one tile when it
+// holds at most big_max particles, else each 64-cell half is one when it
+// holds at most block_max, else each 16-cell quarter when it holds at most
+// half_max, else each octet.  (first, one past last) per tile, in ticket
+// order.  ctr[0] counts tiles; ctr[1] is the CTAs' tile ticket, ctr[2] the
+// deferred count.
 __global__ void k_tile_starts(int n, const uint32_t *__restrict__ skey, const uint2 *__restrict__ cells,
                               uint2 *__restrict__ tiles, uint32_t *ctr, int32_t *globals, uint32_t block_max,
-                              uint32_t half_max) {
+                              uint32_t half_max, uint32_t big_max) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k == 0 && globals) globals[1] = (int32_t)(kDT0 * 1 / kDtMin1);  // density.metal:34-36
     if (k >= n) return;
-    const uint32_t blk = skey[k] >> 6;
-    if (k > 0 && (skey[k - 1] >> 6) == blk) return;
-    uint32_t ofirst[8], oend[8];  // octet ranges; oend == 0 when empty
+    const uint32_t blk = skey[k] >> 7;
+    if (k > 0 && (skey[k - 1] >> 7) == blk) return;
+    uint32_t ofirst[16], oend[16];  // octet ranges; oend == 0 when empty
 #pragma unroll
-    for (int o = 0; o < 8; ++o) {
+    for (int o = 0; o < 16; ++o) {
         uint32_t f = 0xffffffffu, l = 0u;
         for (int j = 0; j < 8; ++j) {
-            const uint2 r = cells[blk * 64u + (uint32_t)(o * 8 + j)];
+            const uint2 r = cells[blk * 128u + (uint32_t)(o * 8 + j)];
             if (r.x != 0xffffffffu) {
                 f = min(f, r.x);
                 l = max(l, r.y + 1u);
@@ -674,19 +676,27 @@ __global__ void k_tile_starts(int n, const uint32_t *__restrict__ skey, const ui
             }
     };
     uint32_t f, l;
-    span(0, 8, f, l);
-    if (l - f <= block_max) {
+    span(0, 16, f, l);
+    if (l - f <= big_max) {
         emit(f, l);
         return;
     }
-    for (int q = 0; q < 4; ++q) {
-        span(2 * q, 2 * q + 2, f, l);
+    for (int hh = 0; hh < 2; ++hh) {
+        span(8 * hh, 8 * hh + 8, f, l);
         if (l <= f) continue;
-        if (l - f <= half_max) {
+        if (l - f <= block_max) {
             emit(f, l);
-        } else {
-            emit(ofirst[2 * q], oend[2 * q]);
-            emit(ofirst[2 * q + 1], oend[2 * q + 1]);
+            continue;
+        }
+        for (int q = 4 * hh; q < 4 * hh + 4; ++q) {
+            span(2 * q, 2 * q + 2, f, l);
+            if (l <= f) continue;
+            if (l - f <= half_max) {
+                emit(f, l);
+            } else {
+                emit(ofirst[2 * q], oend[2 * q]);
+                emit(ofirst[2 * q + 1], oend[2 * q + 1]);
+            }
         }
     }
 }
@@ -2023,7 +2033,7 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     cudaMemsetAsync(ctx->tile_ctr, 0, sizeof(uint32_t) * 4, st);
     k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->cell_sort.keys[ctx->cell_final], ctx->cell_range,
                                                    ctx->tiles, ctx->tile_ctr, ctx->globals, ctx->tile_block_max,
-                                                   ctx->tile_half_max);
+                                                   ctx->tile_half_max, ctx->tile_big_max);
     k_density_tile<<<sms * 2, kTileThreads, sizeof(TileShared), st>>>(a, ctx->tiles, ctx->tile_ctr, ctx->deferred);
     k_density_deferred<kLanesPerParticle><<<sms * 8, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred,
                                                                                            ctx->tile_ctr + 2);
@@ -2068,7 +2078,8 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     uint32_t *ctr = ctx->tile_ctr + 4;
     cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * 4, st);
     k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->cell_sort.keys[ctx->cell_final], ctx->cell_range,
-                                                   ctx->tiles, ctr, nullptr, ctx->tile_block_max, ctx->tile_half_max);
+                                                   ctx->tiles, ctr, nullptr, ctx->tile_block_max, ctx->tile_half_max,
+                                                   ctx->tile_big_max);
     if (kahan) {
         k_acceleration_tile<true><<<sms * 2, kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
                                                                                          ctx->deferred);

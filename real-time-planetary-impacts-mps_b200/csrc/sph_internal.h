@@ -159,8 +159,11 @@ struct sph_ctx {
     uint2 *tiles = nullptr;
     uint32_t *tile_ctr = nullptr;
     uint32_t *deferred = nullptr;
-    // tile sizes: a 64-cell block is one tile up to tile_block_max particles,
-    // else its 16-cell quarters up to tile_half_max, else its octets
+    // tile sizes: a 128-cell block is one tile up to tile_big_max particles
+    // (0: never; measured slower at N = 1e6: such tiles overflow shared memory
+    // and fall back to octets), else its 64-cell halves up to tile_block_max,
+    // else their 16-cell quarters up to tile_half_max, else their octets
+    uint32_t tile_big_max = 0;
     uint32_t tile_block_max = 320;
     uint32_t tile_half_max = 256;
     float2 *eos_forsterite = nullptr, *eos_fe = nullptr;

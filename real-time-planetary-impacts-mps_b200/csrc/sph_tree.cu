@@ -425,3 +425,18 @@ sph_status launch_tree_build(sph_ctx *ctx, cudaStream_t st) {
 }
 
 }  // namespace sph
+
+extern "C" sph_status sph_selftest_tree_capacity(sph_ctx *ctx, void *stream) {
+    using namespace sph;
+    if (!ctx || ctx->params.tree_source != SPH_TREE_GPU) {
+        set_error("sph_selftest_tree_capacity: needs a context with the GPU tree");
+        return SPH_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    const int64_t cap = ctx->tree.tree_cap;
+    ctx->tree.tree_cap = 16;  // room for one branch record at most
+    const sph_status s = launch_tree_build(ctx, (cudaStream_t)stream);
+    ctx->tree.tree_cap = cap;
+    ctx->tree.valid = false;  // the next tree build replaces the partial one
+    return s;
+}

@@ -55,6 +55,24 @@ def test_non_finite_density_is_reported(cuda, pkg):
         c.synchronize()
 
 
+def test_tree_capacity_is_reported_and_context_recovers(cuda, pkg):
+    lib = pkg._lib.load()
+    ic = pkg.ic.make_impact(2048, 512, seed=4)
+    with pkg.Compute(ic, max_children_in_leaf=16) as c:
+        c.step()
+        c.synchronize()
+        want_ok = c.download("pos")
+        assert lib.sph_selftest_tree_capacity(c._h, None) == 0
+        rc = lib.sph_synchronize(c._h, None)
+        assert rc == SPH_ERR_DEVICE_HEALTH, rc
+        assert c.health() & pkg._lib.HEALTH["tree_capacity"]
+        c.clear_health()
+        c.step()  # rebuilds a whole tree
+        c.synchronize()
+        assert np.all(np.isfinite(c.download("pos")))
+        assert not np.array_equal(c.download("pos"), want_ok)  # it stepped
+
+
 def test_async_transfers_round_trip_on_a_stream(cuda, pkg):
     import torch
 
