@@ -493,6 +493,8 @@ def main():
 
     # ---- plain form -------------------------------------------------------
     cp = pkg.Compute(ic, max_children_in_leaf=LEAF, max_tree_depth=DEPTH)
+    cp.hseed_capture(True)  # allocates the density-pass counters; records nothing once off
+    cp.hseed_capture(False)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             cp.step(stream)
@@ -546,6 +548,7 @@ def main():
     log(f"timed: plain {plain_ms / K:.3f} ms/step, chosen {chosen_ms / K:.3f} ms/step")
 
     pp = pass_times(cp, stream, K, "plain_passes")
+    sp = cp.hseed_stats()
     pc = pass_times(cc, stream, K, "chosen_passes")
     st = cc.hseed_stats()
     log("plain  per-pass ms: " + ", ".join(f"{p} {v:.3f}" for p, v in pp.items()))
@@ -617,6 +620,7 @@ def main():
                         "plain": {p: round(v, 4) for p, v in pp.items()}},
             "h_seed": {"sweeps_per_particle": sweeps, "max_sweeps": st["max_sweeps"],
                        "fallback_rate": st["fallbacks"] / max(st["particles"], 1),
+                       "plain_sweeps_per_particle": sp["sweeps"] / max(sp["particles"], 1),
                        "density_tiles": st["tiles"], "density_deferred_particles": st["deferred"],
                        "acceleration_deferred_particles": st["accel_deferred"],
                        "training_ms_per_call": float(np.mean(train_ms)), "adam_steps_per_call": args.train_iters},

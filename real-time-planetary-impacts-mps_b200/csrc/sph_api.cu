@@ -1126,7 +1126,7 @@ sph_status sph_synchronize(sph_ctx *ctx, void *stream) {
     uint32_t w = 0;
     sph_status s = sph_get_health(ctx, &w);
     if (s != SPH_OK) return s;
-    if (w & (SPH_HEALTH_SORT_TIMEOUT | SPH_HEALTH_SCAN_TIMEOUT)) {
+    if (w & (SPH_HEALTH_SORT_TIMEOUT | SPH_HEALTH_SCAN_TIMEOUT | SPH_HEALTH_MLP_TIMEOUT)) {
         set_error("bounded device wait timed out (health 0x%x)", w);
         return SPH_ERR_TIMEOUT;
     }

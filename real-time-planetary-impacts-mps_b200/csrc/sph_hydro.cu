@@ -710,9 +710,10 @@ __global__ void k_tile_starts(int n, const uint32_t *__restrict__ skey, const ui
 // (sorted index) with nothing written; k_density_deferred takes it from the
 // start.  The iteration is density_particle's with the neighbour cache never
 // in use (h < MAX_H throughout, so the reference's int max_h stays 0).
-__device__ __forceinline__ void density_tile_warp(const DensityArgs &a, TileShared &S, uint32_t p0, uint32_t end,
-                                                  int lane, uint16_t (*lists)[kTileList], uint32_t *deferred,
-                                                  uint32_t *dctr) {
+template <class Stage>
+__device__ __forceinline__ void density_tile_warp(const DensityArgs &a, Stage &S, uint32_t *stats, uint32_t p0,
+                                                  uint32_t end, int lane, uint16_t (*lists)[kTileList],
+                                                  uint32_t *deferred, uint32_t *dctr) {
     constexpr int L = kTileLanes;
     constexpr unsigned kFull = 0xffffffffu;
     constexpr int kBig = 0x3fffffff;
@@ -981,10 +982,10 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, TileShar
     if (!live || sub != 0) return;
     if (!gcached) dens += pdens;
     if (a.stats) {
-        atomicAdd(&S.stats[0], (uint32_t)sweeps);
-        if (fell_back) atomicAdd(&S.stats[1], 1u);
-        atomicMax(&S.stats[2], (uint32_t)sweeps);
-        atomicAdd(&S.stats[3], 1u);
+        atomicAdd(&stats[0], (uint32_t)sweeps);
+        if (fell_back) atomicAdd(&stats[1], 1u);
+        atomicMax(&stats[2], (uint32_t)sweeps);
+        atomicAdd(&stats[3], 1u);
     }
     if (a.nn_out) a.nn_out[ind] = (float)nn;
     vdiv = fabsf(vdiv) / dens;
@@ -1162,7 +1163,8 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 if (lane == 0) j = atomicAdd(&S.next, (uint32_t)kTileGpw);
                 j = __shfl_sync(0xffffffffu, j, 0);
                 if (start + j >= end) break;
-                density_tile_warp(a, S, start + j, end, lane, &S.list[(tid >> 5) * kTileGpw], deferred, ctr + 2);
+                density_tile_warp(a, S, S.stats, start + j, end, lane, &S.list[(tid >> 5) * kTileGpw], deferred,
+                              ctr + 2);
             }
             r0 = end;
         }
