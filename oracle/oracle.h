@@ -79,6 +79,23 @@ uint32_t ora_cell_key(float x, float y, float z);
 void ora_gravity_direct_f64(int n, const float *pos3, const float *mass, const int32_t *targets, int nt,
                             double *out);
 
+/* An all-FP64 run of the step (fp64.cpp): FP64 direct-sum gravity, then the
+ * reference's density, acceleration and step passes in double (no
+ * counterpart in the reference; the yardstick of the mixed-precision form). */
+typedef struct {
+    int32_t n;
+    double *pos, *vel, *acc;             /* 3n each */
+    double *rho, *u, *mass, *pressure, *h, *grad_term, *sound_speed, *du, *balsara, *dhdt;
+    int32_t *material, *next_active_time;
+    int32_t *global_time, *dt;           /* scalars, ticks of DT_MIN1 */
+    double *time_s;                      /* scalar, seconds */
+    const float *eos_forsterite, *eos_fe;
+    int32_t eos_res;
+} ora_f64;
+void ora_f64_steps(ora_f64 *st, int n_steps);
+/* kinetic, internal, potential (exact softening), total energy */
+void ora_f64_energy(const ora_f64 *st, double *out);
+
 /* Threads used by the OpenMP loops (0 = library default). */
 void ora_set_threads(int n);
 int ora_get_threads(void);

@@ -46,11 +46,11 @@ class OraState(C.Structure):
 
 def build(force: bool = False) -> str:
     """Compile liboracle.so with the system g++ (OpenMP, no FP contraction)."""
-    src = os.path.join(HERE, "oracle.cpp")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ("oracle.cpp", "fp64.cpp", "oracle.h")]
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(map(os.path.getmtime, srcs)):
         cxx = os.environ.get("SPH_HOST_CXX", "g++")
         cmd = [cxx, "-O3", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
-               "-fno-fast-math", "-o", LIB_PATH + ".tmp", src]
+               "-fno-fast-math", "-o", LIB_PATH + ".tmp"] + srcs[:2]
         subprocess.run(cmd, check=True)
         os.replace(LIB_PATH + ".tmp", LIB_PATH)
     return LIB_PATH
@@ -335,3 +335,64 @@ def last_tree_nodes(n_nodes: int):
     if lib.ora_last_tree_nodes(ptr(poles, _fp), ptr(locs, _fp), n_nodes) < 0:
         raise RuntimeError("no gravity pass with that many nodes")
     return poles, locs
+
+
+class _F64(C.Structure):
+    _dp = C.POINTER(C.c_double)
+    _fields_ = [("n", C.c_int32)] + [(k, C.POINTER(C.c_double)) for k in (
+        "pos", "vel", "acc", "rho", "u", "mass", "pressure", "h", "grad_term", "sound_speed", "du", "balsara",
+        "dhdt")] + [("material", _ip), ("next_active_time", _ip), ("global_time", _ip), ("dt", _ip),
+                    ("time_s", C.POINTER(C.c_double)), ("eos_forsterite", _fp), ("eos_fe", _fp),
+                    ("eos_res", C.c_int32)]
+
+
+class F64Run:
+    """An all-FP64 run of the step from float initial conditions (fp64.cpp):
+    FP64 direct-sum gravity and the reference's SPH passes in double."""
+
+    FIELDS = ("pos", "vel", "acc", "rho", "u", "mass", "pressure", "h", "grad_term", "sound_speed", "du",
+              "balsara", "dhdt")
+
+    def __init__(self, ic: dict, eos_forsterite: np.ndarray, eos_fe: np.ndarray):
+        lib = load("oracle")
+        lib.ora_f64_steps.argtypes = [C.POINTER(_F64), C.c_int]
+        lib.ora_f64_energy.argtypes = [C.POINTER(_F64), C.POINTER(C.c_double)]
+        self.lib = lib
+        n = int(np.asarray(ic["pos"]).reshape(-1, 3).shape[0])
+        self.n = n
+        d = lambda a, k=1: np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1))  # noqa: E731
+        self.a = {f: np.zeros(3 * n if f in ("pos", "vel", "acc") else n, np.float64) for f in self.FIELDS}
+        for f in ("pos", "vel", "rho", "u", "mass", "pressure", "h"):
+            self.a[f][:] = d(ic[f])
+        self.material = np.ascontiguousarray(np.asarray(ic["material"], np.int32).reshape(-1))
+        self.nat = np.zeros(n, np.int32)
+        self.gt = np.zeros(1, np.int32)
+        self.dt = np.zeros(1, np.int32)
+        self.t = np.zeros(1, np.float64)
+        self.eos = (np.ascontiguousarray(eos_forsterite, np.float32), np.ascontiguousarray(eos_fe, np.float32))
+        s = _F64()
+        s.n = n
+        for f in self.FIELDS:
+            setattr(s, f, self.a[f].ctypes.data_as(C.POINTER(C.c_double)))
+        s.material = ptr(self.material, _ip)
+        s.next_active_time = ptr(self.nat, _ip)
+        s.global_time = ptr(self.gt, _ip)
+        s.dt = ptr(self.dt, _ip)
+        s.time_s = self.t.ctypes.data_as(C.POINTER(C.c_double))
+        s.eos_forsterite = ptr(self.eos[0], _fp)
+        s.eos_fe = ptr(self.eos[1], _fp)
+        s.eos_res = int(round((self.eos[0].size // 2) ** 0.5))
+        self.s = s
+
+    def steps(self, k: int):
+        self.lib.ora_f64_steps(C.byref(self.s), int(k))
+
+    def energy(self) -> dict:
+        out = (C.c_double * 4)()
+        self.lib.ora_f64_energy(C.byref(self.s), out)
+        return dict(kinetic=out[0], internal=out[1], potential=out[2], total=out[3])
+
+    def field(self, f: str) -> np.ndarray:
+        a = self.a[f]
+        return a.reshape(-1, 3) if f in ("pos", "vel", "acc") else a
+

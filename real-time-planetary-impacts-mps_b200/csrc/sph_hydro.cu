@@ -21,6 +21,8 @@
 // 1 KiB of local memory.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "sph_internal.h"
 
 namespace sph {
@@ -1982,6 +1984,14 @@ int tile_smem_opt_in() {
     return sms[dev];
 }
 
+// Persistent CTAs of the tile passes: two per SM, but no more than one per
+// ~48 particles (a tile holds ~100-300), so a small context -- an ensemble
+// instance -- leaves the rest of the device to the others.
+unsigned tile_grid(int n, int sms) {
+    const int want = (n + 47) / 48;
+    return (unsigned)std::max(1, std::min(sms * 2, want));
+}
+
 }  // namespace
 
 sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
@@ -2036,8 +2046,9 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->cell_sort.keys[ctx->cell_final], ctx->cell_range,
                                                    ctx->tiles, ctx->tile_ctr, ctx->globals, ctx->tile_block_max,
                                                    ctx->tile_half_max, ctx->tile_big_max);
-    k_density_tile<<<sms * 2, kTileThreads, sizeof(TileShared), st>>>(a, ctx->tiles, ctx->tile_ctr, ctx->deferred);
-    k_density_deferred<kLanesPerParticle><<<sms * 8, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred,
+    const unsigned tgrid = tile_grid(n, sms);
+    k_density_tile<<<tgrid, kTileThreads, sizeof(TileShared), st>>>(a, ctx->tiles, ctx->tile_ctr, ctx->deferred);
+    k_density_deferred<kLanesPerParticle><<<tgrid * 4, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred,
                                                                                            ctx->tile_ctr + 2);
 #endif
     if (ctx->hs.capture) s = launch_hseed_targets(ctx, st);
@@ -2083,15 +2094,15 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
                                                    ctx->tiles, ctr, nullptr, ctx->tile_block_max, ctx->tile_half_max,
                                                    ctx->tile_big_max);
     if (kahan) {
-        k_acceleration_tile<true><<<sms * 2, kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
+        k_acceleration_tile<true><<<tile_grid(n, sms), kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
                                                                                          ctx->deferred);
         k_acceleration_deferred<kLanesPerParticle, true>
-            <<<sms * 8, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
+            <<<tile_grid(n, sms) * 4, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
     } else {
-        k_acceleration_tile<false><<<sms * 2, kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
+        k_acceleration_tile<false><<<tile_grid(n, sms), kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
                                                                                           ctx->deferred);
         k_acceleration_deferred<kLanesPerParticle, false>
-            <<<sms * 8, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
+            <<<tile_grid(n, sms) * 4, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
     }
 #endif
     return cuda_status(cudaGetLastError(), "acceleration");
