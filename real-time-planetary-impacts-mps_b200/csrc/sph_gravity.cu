@@ -32,17 +32,6 @@ struct Pole {
     float4 q0, q1, q2, q3, q4, q5;
 };
 
-__device__ __forceinline__ Pole load_pole(const float4 *poles, int dp) {
-    const float4 *p = poles + (size_t)dp * kPoleQ;
-    Pole r;
-    r.q0 = p[0];
-    r.q1 = p[1];
-    r.q2 = p[2];
-    r.q3 = p[3];
-    r.q4 = p[4];
-    r.q5 = p[5];
-    return r;
-}
 __device__ __forceinline__ void store_pole(float4 *poles, int dp, const Pole &r) {
     float4 *p = poles + (size_t)dp * kPoleQ;
     p[0] = r.q0;

@@ -2,8 +2,9 @@
 // MLP that predicts, from a particle's state at the start of the density
 // pass, the smoothing length the density iteration (density.metal:73-143)
 // converges to.  The prediction only seeds that iteration; the iteration's
-// own test still decides convergence, and a seed whose first sweep disagrees
-// with it by more than kSeedFallback falls back to the plain initial guess.
+// own test still decides convergence, and a seed whose first sweep moves h by
+// more than 5 % falls back to the plain initial guess (the density kernels,
+// sph_hydro.cu).
 // No counterpart in the reference.
 //
 // Features (per particle, before the pass): log h0, (dh/dt) dt / h0, the last
@@ -45,7 +46,6 @@ constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kHid * kIn, kOffW2 = kOffB1 + kHid, 
 // normalisation block: feature mean [8], feature 1/deviation [8], target mean, target deviation
 constexpr int kNorm = 2 * kIn + 2;
 constexpr int kTile = 128;
-constexpr float kSeedFallback = 0.05f;
 constexpr int kMbarLimit = 1 << 24;
 
 // shared-memory map of the MLP kernel (bytes)
