@@ -574,7 +574,10 @@ constexpr int kTileGroups = kTileThreads / kTileLanes;      // particles in flig
 constexpr int kTileStageMax = 3840;                         // staged particles per tile
 constexpr int kTileCellsMax = 1024;                         // cells of a tile's staged box
 constexpr int kTileCellsPerThread = (kTileCellsMax + kTileThreads - 1) / kTileThreads;
-constexpr int kTileReach = 3;                               // cells a list box may extend past its own cell
+#ifndef SPH_TILE_REACH_CELLS
+#define SPH_TILE_REACH_CELLS 3
+#endif
+constexpr int kTileReach = SPH_TILE_REACH_CELLS;            // cells a list box may extend past its own cell
 constexpr int kTileList = 256;                              // list entries per particle (staged slots)
 #ifndef SPH_TILE_LIST_REACH
 #define SPH_TILE_LIST_REACH 1.05f
