@@ -623,6 +623,8 @@ def main():
                        "plain_sweeps_per_particle": sp["sweeps"] / max(sp["particles"], 1),
                        "density_tiles": st["tiles"], "density_deferred_particles": st["deferred"],
                        "acceleration_deferred_particles": st["accel_deferred"],
+                       "density_coarse_tiles": st["coarse_tiles"],
+                       "acceleration_coarse_tiles": st["accel_coarse_tiles"],
                        "training_ms_per_call": float(np.mean(train_ms)), "adam_steps_per_call": args.train_iters},
             "roofline": {"bound": "hbm", "kernel": f"{dom} pass ({PASS_KERNELS[dom]}), chosen form",
                          "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",

@@ -187,6 +187,24 @@ void sph_form_default(sph_form *f); /* reference form, theta 0.5 */
 sph_status sph_set_form(sph_ctx *ctx, const sph_form *f);
 sph_status sph_get_form(const sph_ctx *ctx, sph_form *f);
 
+/* Tiling of the product build's density and acceleration passes.  It changes
+ * how the work is scheduled, not what is computed (up to the float summation
+ * order).  A 128-cell block of the sorted particles is one tile when it holds
+ * at most big_max particles (0: never), else each 64-cell half is one up to
+ * block_max, else each 16-cell quarter up to half_max, else each octet.
+ * coarse != 0 runs the particles whose neighbour boxes reach more than 3 cells
+ * past their own in coarse tiles (512-cell blocks staged by 4 x 4 x 4-cell
+ * units); coarse = 0 hands them to the per-particle walk.  The parity build
+ * (one lane per particle) ignores the tiling.  Drops a captured step graph. */
+typedef struct {
+    uint32_t big_max;   /* default 0 */
+    uint32_t block_max; /* default 320 */
+    uint32_t half_max;  /* default 256 */
+    int32_t coarse;     /* default 1 */
+} sph_tiling;
+sph_status sph_set_tiling(sph_ctx *ctx, const sph_tiling *t);
+sph_status sph_get_tiling(const sph_ctx *ctx, sph_tiling *t);
+
 /* FP64 direct-sum gravity at n_targets particles (host array of particle
  * indices), from the current positions and masses of all particles, with the
  * cubic-spline softened kernel and its exact coefficients: out receives
@@ -223,9 +241,12 @@ typedef struct {
     uint32_t fallbacks;  /* particles whose learned seed was abandoned */
     uint32_t max_sweeps; /* most sweeps of one particle */
     uint32_t particles;  /* particles iterated */
-    uint32_t tiles;      /* occupied cell octets the product build's density pass staged */
+    uint32_t tiles;      /* cell tiles the product build's density pass staged */
     uint32_t deferred;   /* particles it handed from the tiles to the per-particle walk */
     uint32_t accel_deferred; /* the same count of the last acceleration pass */
+    uint32_t coarse_tiles;   /* coarse tiles (512-cell blocks) of the density pass: blocks
+                                holding particles whose boxes reach past the cell tiles */
+    uint32_t accel_coarse_tiles; /* the same count of the last acceleration pass */
 } sph_hseed_stats;
 int32_t sph_hseed_num_params(void);
 sph_status sph_hseed_capture(sph_ctx *ctx, int32_t on);

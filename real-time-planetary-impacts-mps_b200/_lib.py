@@ -76,6 +76,10 @@ class SphForm(C.Structure):
                 ("h_tolerance", C.c_float), ("timestep", C.c_int32)]
 
 
+class SphTiling(C.Structure):
+    _fields_ = [("big_max", C.c_uint32), ("block_max", C.c_uint32), ("half_max", C.c_uint32), ("coarse", C.c_int32)]
+
+
 class SphEnsembleTuning(C.Structure):
     _fields_ = [("max_children_in_leaf", C.c_int32), ("tile_block_max", C.c_uint32), ("ms_per_step", C.c_float),
                 ("gravity_median_error", C.c_float)]
@@ -84,7 +88,8 @@ class SphEnsembleTuning(C.Structure):
 class SphHSeedStats(C.Structure):
     _fields_ = [("sweeps", C.c_uint32), ("fallbacks", C.c_uint32), ("max_sweeps", C.c_uint32),
                 ("particles", C.c_uint32), ("tiles", C.c_uint32), ("deferred", C.c_uint32),
-                ("accel_deferred", C.c_uint32)]
+                ("accel_deferred", C.c_uint32), ("coarse_tiles", C.c_uint32),
+                ("accel_coarse_tiles", C.c_uint32)]
 
 
 SPH_HSEED_PLAIN = 0
@@ -189,6 +194,8 @@ def load(parity: bool = False) -> C.CDLL:
         "sph_form_default": (None, [C.POINTER(SphForm)]),
         "sph_set_form": (st, [vp, C.POINTER(SphForm)]),
         "sph_get_form": (st, [vp, C.POINTER(SphForm)]),
+        "sph_set_tiling": (st, [vp, C.POINTER(SphTiling)]),
+        "sph_get_tiling": (st, [vp, C.POINTER(SphTiling)]),
         "sph_gravity_direct_f64": (st, [vp, _ip, C.c_int32, C.POINTER(C.c_double), vp]),
         "sph_diagnostics": (st, [vp, vp, C.c_float, C.POINTER(SphDiag)]),
         "sph_hseed_num_params": (C.c_int32, []),

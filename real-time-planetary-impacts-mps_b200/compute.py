@@ -246,6 +246,29 @@ class Compute:
                     h_seed="learned" if f.h_seed == _lib.SPH_HSEED_LEARNED else "plain", h_tolerance=f.h_tolerance,
                     timestep="individual" if f.timestep == 1 else "global")
 
+    def set_tiling(self, big_max: int | None = None, block_max: int | None = None, half_max: int | None = None,
+                   coarse: bool | None = None):
+        """Scheduling of the density and acceleration passes (sph_set_tiling):
+        tile sizes in particles, and whether particles whose neighbour boxes
+        reach past 3 cells run in coarse tiles (True) or in the per-particle
+        walk (False).  Arguments left at None keep their current value."""
+        t = _lib.SphTiling()
+        self._check(self._lib.sph_get_tiling(self._h, C.byref(t)), "sph_get_tiling")
+        if big_max is not None:
+            t.big_max = int(big_max)
+        if block_max is not None:
+            t.block_max = int(block_max)
+        if half_max is not None:
+            t.half_max = int(half_max)
+        if coarse is not None:
+            t.coarse = 1 if coarse else 0
+        self._check(self._lib.sph_set_tiling(self._h, C.byref(t)), "sph_set_tiling")
+
+    def get_tiling(self) -> dict:
+        t = _lib.SphTiling()
+        self._check(self._lib.sph_get_tiling(self._h, C.byref(t)), "sph_get_tiling")
+        return dict(big_max=t.big_max, block_max=t.block_max, half_max=t.half_max, coarse=bool(t.coarse))
+
     # ---- learned smoothing-length seed (no reference counterpart) ------
     def hseed_capture(self, on: bool = True):
         """Record (features, converged h) of every following density pass."""
@@ -300,7 +323,8 @@ class Compute:
         st = _lib.SphHSeedStats()
         self._check(self._lib.sph_hseed_get_stats(self._h, C.byref(st)), "sph_hseed_get_stats")
         return dict(sweeps=st.sweeps, fallbacks=st.fallbacks, max_sweeps=st.max_sweeps, particles=st.particles,
-                    tiles=st.tiles, deferred=st.deferred, accel_deferred=st.accel_deferred)
+                    tiles=st.tiles, deferred=st.deferred, accel_deferred=st.accel_deferred,
+                    coarse_tiles=st.coarse_tiles, accel_coarse_tiles=st.accel_coarse_tiles)
 
     def diagnostics(self, stream=None, theta_potential: float = 0.5) -> dict:
         """FP64 conservation sums (mass, energies, momentum, angular momentum)."""

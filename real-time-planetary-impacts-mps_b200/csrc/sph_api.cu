@@ -306,7 +306,7 @@ sph_status sph_destroy(sph_ctx *ctx) {
                     ctx->du, ctx->B, ctx->dhdt, ctx->gnorm, ctx->phi, ctx->mat, ctx->nat, ctx->active, ctx->globals,
                     ctx->health, ctx->cell_range, ctx->sp4, ctx->sv4, ctx->sA, ctx->sB, ctx->sC,
                     ctx->eos_forsterite, ctx->eos_fe, ctx->stage, ctx->snapshot, ctx->pos64, ctx->dglob,
-                    ctx->diag, ctx->tiles, ctx->tile_ctr, ctx->deferred};
+                    ctx->diag, ctx->tiles, ctx->tile_ctr, ctx->deferred, ctx->units, ctx->coarse_flags};
     for (void *b : bufs) cudaFree(b);
     sort_free(ctx->cell_sort);
     hseed_free(ctx);
@@ -383,8 +383,11 @@ sph_status sph_create(const sph_params *params, const sph_ic *ic, sph_ctx **out)
     chk(dmalloc(&ctx->dglob, 4));
     chk(dmalloc(&ctx->diag, (size_t)kDiagDoubles));
     chk(dmalloc(&ctx->tiles, (size_t)n));
-    chk(dmalloc(&ctx->tile_ctr, 8));
+    chk(dmalloc(&ctx->tile_ctr, 16));
     chk(dmalloc(&ctx->deferred, (size_t)n));
+    chk(dmalloc(&ctx->units, (size_t)kNumUnits));
+    chk(dmalloc(&ctx->coarse_flags, (size_t)kNumCoarseBlocks));
+    if (e == cudaSuccess) e = cudaMemset(ctx->coarse_flags, 0, kNumCoarseBlocks);
     if (e != cudaSuccess) {
         s = cuda_status(e, "sph_create allocation");
         sph_destroy(ctx);
@@ -950,6 +953,36 @@ sph_status sph_set_form(sph_ctx *ctx, const sph_form *f) {
 sph_status sph_get_form(const sph_ctx *ctx, sph_form *f) {
     if (!ctx || !f) return SPH_ERR_INVALID_ARG;
     *f = ctx->form;
+    return SPH_OK;
+}
+
+sph_status sph_set_tiling(sph_ctx *ctx, const sph_tiling *t) {
+    if (!ctx || !t) return SPH_ERR_INVALID_ARG;
+    constexpr uint32_t kMaxTile = 1u << 20;
+    if (t->block_max < 1 || t->block_max > kMaxTile || t->half_max < 1 || t->half_max > kMaxTile ||
+        t->big_max > kMaxTile) {
+        set_error("sph_set_tiling: block_max and half_max must be in [1, %u], big_max in [0, %u]", kMaxTile,
+                  kMaxTile);
+        return SPH_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    if (ctx->graph) {
+        cudaGraphExecDestroy(ctx->graph);
+        ctx->graph = nullptr;
+    }
+    ctx->tile_big_max = t->big_max;
+    ctx->tile_block_max = t->block_max;
+    ctx->tile_half_max = t->half_max;
+    ctx->tile_coarse = t->coarse ? 1 : 0;
+    return SPH_OK;
+}
+
+sph_status sph_get_tiling(const sph_ctx *ctx, sph_tiling *t) {
+    if (!ctx || !t) return SPH_ERR_INVALID_ARG;
+    t->big_max = ctx->tile_big_max;
+    t->block_max = ctx->tile_block_max;
+    t->half_max = ctx->tile_half_max;
+    t->coarse = ctx->tile_coarse;
     return SPH_OK;
 }
 

@@ -83,6 +83,15 @@ __device__ __forceinline__ uint32_t cell_index_of(int x, int y, int z) {
     const int mask = kCellsPerDim - 1;
     return morton3((uint32_t)(x & mask), (uint32_t)(y & mask), (uint32_t)(z & mask));
 }
+// Coarse units: 4 x 4 x 4 cells, the cells whose keys agree above the low six
+// bits (unit index = cell key >> 6); 512-cell blocks are 2 x 2 x 2 units.
+constexpr int kUnitShift = 2;  // cells per unit edge = 1 << kUnitShift
+constexpr uint32_t kNumUnits = kNumCells >> (3 * kUnitShift);
+constexpr uint32_t kNumCoarseBlocks = kNumUnits >> 3;
+__device__ __forceinline__ uint32_t unit_index_of(int x, int y, int z) {
+    const int mask = (kCellsPerDim >> kUnitShift) - 1;
+    return morton3((uint32_t)(x & mask), (uint32_t)(y & mask), (uint32_t)(z & mask));
+}
 struct CellBox {
     int lo0, lo1, lo2, hi0, hi1, hi2;
 };

@@ -661,13 +661,15 @@ sph_status sph_hseed_get_stats(sph_ctx *ctx, sph_hseed_stats *out) {
     if (!ctx || !out) return SPH_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     std::memset(out, 0, sizeof(*out));
-    uint32_t v[4] = {0, 0, 0, 0}, t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t v[4] = {0, 0, 0, 0}, t[16] = {};
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess && ctx->tile_ctr) e = cudaMemcpy(t, ctx->tile_ctr, sizeof(t), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_status(e, "sph_hseed_get_stats");
     out->tiles = t[0];
     out->deferred = t[2];
-    out->accel_deferred = t[6];
+    out->accel_deferred = t[10];
+    out->coarse_tiles = t[4];
+    out->accel_coarse_tiles = t[12];
     if (!ctx->hs.stats) return SPH_OK;
     e = cudaMemcpy(v, ctx->hs.stats, sizeof(v), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_status(e, "sph_hseed_get_stats");

@@ -263,6 +263,9 @@ struct DensityArgs {
     const uint32_t *cidx;
     const uint32_t *skey;  // sorted cell keys (tile passes)
     const uint2 *cells;
+    const uint2 *units;    // 64-cell unit ranges (coarse tiles)
+    uint8_t *cflags;       // per 512-cell block: holds a coarse-tile particle
+    int coarse;            // coarse tiles on
     const float4 *sp4, *sv4;
     float *h, *rho, *f, *P, *c, *B;
     const float *u;
@@ -603,12 +606,11 @@ struct TileShared {
     int defer_all;
 };
 
-// The list box of a tile particle at smoothing length hb -- the cells within
-// 2 hb kTileListReach, widened by 1e-3 of a cell so that float rounding of the
-// cell coordinates (|x| / CELL_WIDTH < 2^12, a few 1e-4 of a cell) never drops
-// a cell -- and whether the tile path can take the particle (reach within
-// kTileReach cells of its own, h < MAX_H).
-__device__ __forceinline__ bool tile_box(float px, float py, float pz, float hb, CellBox &b,
+// The list box of a tile particle at smoothing length hb: the cells within
+// 2 hb reach, widened by 1e-3 of a cell so that float rounding of the cell
+// coordinates (|x| / CELL_WIDTH < 2^12, a few 1e-4 of a cell) never drops a
+// cell.
+__device__ __forceinline__ void tile_box(float px, float py, float pz, float hb, CellBox &b,
                                          float reach = kTileListReach) {
     constexpr float iw = 1.f / kCellWidth;
     constexpr float widen = 1e-3f;
@@ -619,9 +621,40 @@ __device__ __forceinline__ bool tile_box(float px, float py, float pz, float hb,
     b.hi0 = (int)floorf((px + rl) * iw + widen);
     b.hi1 = (int)floorf((py + rl) * iw + widen);
     b.hi2 = (int)floorf((pz + rl) * iw + widen);
+}
+
+// The (first, last) sorted range of tiling unit (x, y, z): a cell (U = 0) or a
+// 64-cell unit (U = kUnitShift); first is 0xffffffff when it is empty.
+template <int U>
+__device__ __forceinline__ uint2 unit_range(const uint2 *cells, const uint2 *units, int x, int y, int z) {
+    if (U == 0) return __ldg(cells + cell_index_of(x, y, z));
+    return __ldg(units + unit_index_of(x, y, z));
+}
+
+// Whether a cell box reaches at most kTileReach tiling units (cells for U = 0,
+// 64-cell units for U = kUnitShift) past the unit of cell (ox, oy, oz).
+template <int U>
+__device__ __forceinline__ bool within_reach(int ox, int oy, int oz, const CellBox &b) {
+    return (ox >> U) - (b.lo0 >> U) <= kTileReach && (b.hi0 >> U) - (ox >> U) <= kTileReach &&
+           (oy >> U) - (b.lo1 >> U) <= kTileReach && (b.hi1 >> U) - (oy >> U) <= kTileReach &&
+           (oz >> U) - (b.lo2 >> U) <= kTileReach && (b.hi2 >> U) - (oz >> U) <= kTileReach;
+}
+
+// The pass that takes a density particle whose iteration starts from list
+// radius 2 hb kTileListReach: 0 the cell tiles, kUnitShift the coarse tiles
+// (a box past kTileReach cells, within kTileReach units), -1 the per-particle
+// pass (h at MAX_H, where the reference's neighbour cache comes into play, or
+// coarse tiles off).  Every pass evaluates it from the same inputs, so each
+// particle is taken by exactly one.
+__device__ __forceinline__ int density_mode(float px, float py, float pz, float hb, int coarse) {
+    if (!(hb < kMaxH)) return -1;
+    constexpr float iw = 1.f / kCellWidth;
+    CellBox b;
+    tile_box(px, py, pz, hb, b);
     const int ox = (int)floorf(px * iw), oy = (int)floorf(py * iw), oz = (int)floorf(pz * iw);
-    return hb < kMaxH && ox - b.lo0 <= kTileReach && b.hi0 - ox <= kTileReach && oy - b.lo1 <= kTileReach &&
-           b.hi1 - oy <= kTileReach && oz - b.lo2 <= kTileReach && b.hi2 - oz <= kTileReach;
+    if (within_reach<0>(ox, oy, oz, b)) return 0;
+    if (coarse && within_reach<kUnitShift>(ox, oy, oz, b)) return kUnitShift;
+    return -1;
 }
 
 // The starting h of an active particle's iteration (the learned seed when it
@@ -706,8 +739,29 @@ __global__ void k_tile_starts(int n, const uint32_t *__restrict__ skey, const ui
     }
 }
 
+// Coarse tiles: at the first sorted particle of every 512-cell block (2 x 2 x
+// 2 units) that a cell-tile pass flagged, the block's (first, one past last)
+// sorted range; the flag is cleared for the next pass.  ctr[0] counts tiles.
+__global__ void k_coarse_starts(int n, const uint32_t *__restrict__ skey, const uint2 *__restrict__ units,
+                                uint8_t *__restrict__ flags, uint2 *__restrict__ tiles, uint32_t *ctr) {
+    constexpr int kShift = 3 * kUnitShift + 3;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t blk = skey[k] >> kShift;
+    if (k > 0 && (skey[k - 1] >> kShift) == blk) return;
+    if (!flags[blk]) return;
+    flags[blk] = 0;
+    uint32_t l = (uint32_t)k + 1u;
+    for (int j = 0; j < 8; ++j) {
+        const uint2 r = units[blk * 8u + (uint32_t)j];
+        if (r.x != 0xffffffffu) l = max(l, r.y + 1u);
+    }
+    tiles[atomicAdd(ctr, 1u)] = make_uint2((uint32_t)k, l);
+}
+
 // One warp: the density pass of sorted particles p0 .. p0 + 3 of the staged
-// tile (lane group g = lane / 8 takes p0 + g), in lockstep so the warp never
+// tile (lane group g = lane / 8 takes p0 + g) whose pass is U (0 cell tiles,
+// kUnitShift coarse tiles; the staged box counts U-units), in lockstep so the warp never
 // runs its groups one after another: the list build is transposed (each lane
 // takes one staged slot of a row and tests it against all four particles), and
 // the sweeps run over the longest of the four lists with the others predicated
@@ -715,7 +769,7 @@ __global__ void k_tile_starts(int n, const uint32_t *__restrict__ skey, const ui
 // (sorted index) with nothing written; k_density_deferred takes it from the
 // start.  The iteration is density_particle's with the neighbour cache never
 // in use (h < MAX_H throughout, so the reference's int max_h stays 0).
-template <class Stage>
+template <int U, class Stage>
 __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, Stage &S, uint32_t *stats, uint32_t p0,
                                                   uint32_t end, int lane, uint16_t (*lists)[kTileList],
                                                   uint32_t *deferred, uint32_t *dctr) {
@@ -733,8 +787,8 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, Stage &S
         me = a.sp4[p];
         mv = a.sv4[p];
         if (!a.active[ind]) {
-            // density.metal:40-55: EOS only
-            if (sub == 0) {
+            // density.metal:40-55: EOS only (in the cell-tile pass)
+            if (U == 0 && sub == 0) {
                 float2 pc = eos_lookup(a.eos, a.mat[ind], a.rho[ind], a.u[ind]);
                 a.P[ind] = pc.x;
                 a.c[ind] = pc.y;
@@ -756,8 +810,13 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, Stage &S
     if (live) {
         h_plain = a.h[ind];
         hi = tile_start_h(a, ind, h_plain, seeded);
-        CellBox b;
-        if (S.defer_all || !tile_box(px, py, pz, fmaxf(hi, h_plain), b)) defer();
+        const int m = density_mode(px, py, pz, fmaxf(hi, h_plain), a.coarse);
+        if (m != U) {
+            if (U == 0 && m < 0) defer();
+            else live = false;  // another tile pass takes it
+        } else if (S.defer_all) {
+            defer();
+        }
     }
     const int lo0 = S.box[0], lo1 = S.box[1], lo2 = S.box[2];
     const int ny = S.box[4] - lo1 + 1, nz = S.box[5] - lo2 + 1;
@@ -767,8 +826,10 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, Stage &S
     auto build = [&](bool want, float hb) {
         CellBox b;
         if (want) {
-            if (!tile_box(px, py, pz, hb, b) || b.lo0 < lo0 || b.lo1 < lo1 || b.lo2 < lo2 || b.hi0 > S.box[3] ||
-                b.hi1 > S.box[4] || b.hi2 > S.box[5]) {
+            tile_box(px, py, pz, hb, b);
+            b.lo0 >>= U, b.lo1 >>= U, b.lo2 >>= U, b.hi0 >>= U, b.hi1 >>= U, b.hi2 >>= U;  // U-units
+            if (!(hb < kMaxH) || b.lo0 < lo0 || b.lo1 < lo1 || b.lo2 < lo2 || b.hi0 > S.box[3] || b.hi1 > S.box[4] ||
+                b.hi2 > S.box[5]) {
                 defer();
                 want = false;
             }
@@ -807,16 +868,19 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, Stage &S
             uint32_t len = 0u, s0 = 0u;
             if (r < rows) {
                 const int x = u0 + r / nyu, y = u1 + r % nyu;
+                // the row's extent in x and y
+                const float x0 = (float)(x * (1 << U)) * w, x1 = (float)((x + 1) * (1 << U)) * w;
+                const float y0 = (float)(y * (1 << U)) * w, y1 = (float)((y + 1) * (1 << U)) * w;
                 int zl = 0x3fffffff, zh = -0x3fffffff;
 #pragma unroll
                 for (int k = 0; k < kTileGpw; ++k) {
-                    const float gx = fmaxf(fmaxf((float)x * w - qx[k], qx[k] - (float)(x + 1) * w) - kCellMargin, 0.f);
-                    const float gy = fmaxf(fmaxf((float)y * w - qy[k], qy[k] - (float)(y + 1) * w) - kCellMargin, 0.f);
+                    const float gx = fmaxf(fmaxf(x0 - qx[k], qx[k] - x1) - kCellMargin, 0.f);
+                    const float gy = fmaxf(fmaxf(y0 - qy[k], qy[k] - y1) - kCellMargin, 0.f);
                     const float g2 = gx * gx + gy * gy;
                     if (g2 <= qr[k]) {
                         const float dz = sqrtf(qr[k] - g2);
-                        zl = min(zl, (int)floorf((qz[k] - dz) * iw - 1e-3f));
-                        zh = max(zh, (int)floorf((qz[k] + dz) * iw + 1e-3f));
+                        zl = min(zl, (int)floorf((qz[k] - dz) * iw - 1e-3f) >> U);
+                        zh = max(zh, (int)floorf((qz[k] + dz) * iw + 1e-3f) >> U);
                     }
                 }
                 zl = max(zl, u2);
@@ -1010,8 +1074,15 @@ __device__ __forceinline__ void density_tile_warp(const DensityArgs &a, Stage &S
     a.sC[p] = make_float4(mi, (fi * pc.x / (dens * dens)), dens, bal);
 }
 
+// The density tile pass U over the tiles of `tiles` (ctr[0] of them, ctr[1]
+// the tile ticket): U = 0 the cell tiles, whose staged box counts cells;
+// U = kUnitShift the coarse tiles (512-cell blocks), whose staged box counts
+// 64-cell units.  Deferred particles are appended to `deferred`, counted in
+// *dctr.
+template <int U>
 __global__ void __launch_bounds__(kTileThreads, 2)
-    k_density_tile(DensityArgs a, const uint2 *__restrict__ tiles, uint32_t *ctr, uint32_t *__restrict__ deferred) {
+    k_density_tile(DensityArgs a, const uint2 *__restrict__ tiles, uint32_t *ctr, uint32_t *__restrict__ deferred,
+                   uint32_t *dctr) {
     extern __shared__ float4 s_tile_raw[];
     TileShared &S = *reinterpret_cast<TileShared *>(s_tile_raw);
     const int tid = threadIdx.x, lane = tid & 31;
@@ -1032,21 +1103,26 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         if (S.tile >= ntiles) break;
         const uint32_t tstart = S.start, tend = S.end;
         // a tile whose staged box overflows shared memory is taken again as
-        // its octets, one at a time; an octet that still overflows is handed
-        // to the per-particle pass
-        const bool splittable = (a.skey[tstart] >> 3) != (a.skey[tend - 1] >> 3);
+        // its octets (coarse tiles: its units), one at a time; one that still
+        // overflows is handed to the per-particle pass
+        constexpr int kSplit = U == 0 ? 3 : 3 * U;
+        const bool splittable = (a.skey[tstart] >> kSplit) != (a.skey[tend - 1] >> kSplit);
         bool whole = true;
         uint32_t r0 = tstart;
         while (r0 < tend) {
             __syncthreads();
             if (tid == 0) {
                 uint32_t r1 = tend;
-                if (!whole) {  // the rest of r0's octet
-                    const uint32_t o = a.skey[r0] >> 3;
+                if (!whole) {  // the rest of r0's octet / unit
+                    const uint32_t o = a.skey[r0] >> kSplit;
                     r1 = r0 + 1u;
-                    for (int j = 0; j < 8; ++j) {
-                        const uint2 r = a.cells[o * 8u + (uint32_t)j];
-                        if (r.x != 0xffffffffu) r1 = max(r1, r.y + 1u);
+                    if (U == 0) {
+                        for (int j = 0; j < 8; ++j) {
+                            const uint2 r = a.cells[o * 8u + (uint32_t)j];
+                            if (r.x != 0xffffffffu) r1 = max(r1, r.y + 1u);
+                        }
+                    } else {
+                        r1 = max(r1, a.units[o].y + 1u);
                     }
                 }
                 S.end = r1;
@@ -1067,15 +1143,18 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                     const float h_plain = a.h[ind];
                     bool seeded;
                     const float h0 = tile_start_h(a, ind, h_plain, seeded);
+                    const float hb = fmaxf(h0, h_plain);
+                    const int m = density_mode(me.x, me.y, me.z, hb, a.coarse);
+                    if (U == 0 && m == kUnitShift) a.cflags[a.skey[p] >> (3 * kUnitShift + 3)] = 1;
+                    if (m != U) continue;
                     CellBox cb;
-                    if (!tile_box(me.x, me.y, me.z, fmaxf(h0, h_plain), cb)) continue;
-                    tile_box(me.x, me.y, me.z, fmaxf(h0, h_plain), cb, fmaxf(kTileStageReach, kTileListReach));
-                    b[0] = min(b[0], cb.lo0);
-                    b[1] = min(b[1], cb.lo1);
-                    b[2] = min(b[2], cb.lo2);
-                    b[3] = max(b[3], cb.hi0);
-                    b[4] = max(b[4], cb.hi1);
-                    b[5] = max(b[5], cb.hi2);
+                    tile_box(me.x, me.y, me.z, hb, cb, fmaxf(kTileStageReach, kTileListReach));
+                    b[0] = min(b[0], cb.lo0 >> U);
+                    b[1] = min(b[1], cb.lo1 >> U);
+                    b[2] = min(b[2], cb.lo2 >> U);
+                    b[3] = max(b[3], cb.hi0 >> U);
+                    b[4] = max(b[4], cb.hi1 >> U);
+                    b[5] = max(b[5], cb.hi2 >> U);
                 }
     #pragma unroll
                 for (int k = 0; k < 3; ++k) {
@@ -1113,7 +1192,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 c_cnt[k] = 0u;
                 if (c < ncell) {
                     const int ix = c / (ny * nz), rem = c - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
-                    const uint2 r = __ldg(a.cells + cell_index_of(lo0 + ix, lo1 + iy, lo2 + iz));
+                    const uint2 r = unit_range<U>(a.cells, a.units, lo0 + ix, lo1 + iy, lo2 + iz);
                     if (r.x != 0xffffffffu) {
                         c_cnt[k] = r.y - r.x + 1u;
                         S.first[c] = r.x;
@@ -1168,8 +1247,8 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 if (lane == 0) j = atomicAdd(&S.next, (uint32_t)kTileGpw);
                 j = __shfl_sync(0xffffffffu, j, 0);
                 if (start + j >= end) break;
-                density_tile_warp(a, S, S.stats, start + j, end, lane, &S.list[(tid >> 5) * kTileGpw], deferred,
-                              ctr + 2);
+                density_tile_warp<U>(a, S, S.stats, start + j, end, lane, &S.list[(tid >> 5) * kTileGpw], deferred,
+                                     dctr);
             }
             r0 = end;
         }
@@ -1189,6 +1268,9 @@ struct AccelArgs {
     const uint32_t *cidx;
     const uint32_t *skey;  // sorted cell keys (tile passes)
     const uint2 *cells;
+    const uint2 *units;    // 64-cell unit ranges (coarse tiles)
+    uint8_t *cflags;       // per 512-cell block: holds a coarse-tile particle
+    int coarse;            // coarse tiles on
     const float4 *sA, *sB, *sC;
     float4 *acc4;
     float *du, *dhdt;
@@ -1440,20 +1522,26 @@ struct TileAccShared {
     int hmax_bits;                      // largest staged h (float bits; h > 0)
 };
 
-// The reference's box of an acceleration particle and whether the tile path
-// can take it (reach within kTileReach cells of its own, h < MAX_H).
-__device__ __forceinline__ bool accel_box(float px, float py, float pz, float h, CellBox &b) {
+// The reference's box of an acceleration particle (cells) and the pass that
+// takes it: 0 the cell tiles (reach within kTileReach cells of its own),
+// kUnitShift the coarse tiles (within kTileReach units), -1 the per-particle
+// pass (h at MAX_H, or coarse tiles off).
+__device__ __forceinline__ int accel_mode(float px, float py, float pz, float h, CellBox &b, int coarse) {
     b = cell_box(px, py, pz, fmin_ref(h, kMaxH));
+    if (!(h < kMaxH)) return -1;
     const int ox = (int)floorf(__fdiv_rn(px, kCellWidth)), oy = (int)floorf(__fdiv_rn(py, kCellWidth)),
               oz = (int)floorf(__fdiv_rn(pz, kCellWidth));
-    return h < kMaxH && ox - b.lo0 <= kTileReach && b.hi0 - ox <= kTileReach && oy - b.lo1 <= kTileReach &&
-           b.hi1 - oy <= kTileReach && oz - b.lo2 <= kTileReach && b.hi2 - oz <= kTileReach;
+    if (within_reach<0>(ox, oy, oz, b)) return 0;
+    if (coarse && within_reach<kUnitShift>(ox, oy, oz, b)) return kUnitShift;
+    return -1;
 }
 
 // One warp: the acceleration pass of sorted particles p0 .. p0 + 3 of the
-// staged tile (lane group g takes p0 + g).  Returns the warp's smallest
-// timestep in ticks (INT_MAX when none).
-template <bool KAHAN>
+// staged tile (lane group g takes p0 + g) whose pass is U (the staged box
+// counts U-units; the group boxes and staged cells stay in cells, relative to
+// the box's first cell).  Returns the warp's smallest timestep in ticks
+// (INT_MAX when none).
+template <bool KAHAN, int U>
 __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared &S, uint32_t p0, uint32_t end,
                                                int lane, int wslot, uint32_t *deferred, uint32_t *dctr) {
     constexpr int L = kTileLanes;
@@ -1468,7 +1556,7 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
     if (live) {
         ind = a.cidx[p];
         live = a.active[ind] != 0;
-        if (!live) idt_inactive = inactive_ticks(a, ind);
+        if (!live && U == 0) idt_inactive = inactive_ticks(a, ind);
     }
     float4 A = make_float4(0.f, 0.f, 0.f, 1.f), Bv = A, Cv = A;
     if (live) {
@@ -1482,7 +1570,11 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
     CellBox b;
     bool want = false;
     if (live) {
-        if (S.defer_all || !accel_box(I.xi, I.yi, I.zi, I.hi, b)) {
+        const int m = accel_mode(I.xi, I.yi, I.zi, I.hi, b, a.coarse);
+        if (m != U) {
+            if (U == 0 && m < 0 && sub == 0) deferred[atomicAdd(dctr, 1u)] = p;
+            live = false;  // deferred, or another tile pass takes it
+        } else if (S.defer_all) {
             if (sub == 0) deferred[atomicAdd(dctr, 1u)] = p;
             live = false;
         } else {
@@ -1495,17 +1587,17 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
     }
     if (want && sub == 0) {
         int *gb = S.gbox[wslot * kTileGpw + g];
-        gb[0] = b.lo0 - lo0;
-        gb[1] = b.lo1 - lo1;
-        gb[2] = b.lo2 - lo2;
-        gb[3] = b.hi0 - lo0;
-        gb[4] = b.hi1 - lo1;
-        gb[5] = b.hi2 - lo2;
+        gb[0] = b.lo0 - lo0 * (1 << U);
+        gb[1] = b.lo1 - lo1 * (1 << U);
+        gb[2] = b.lo2 - lo2 * (1 << U);
+        gb[3] = b.hi0 - lo0 * (1 << U);
+        gb[4] = b.hi1 - lo1 * (1 << U);
+        gb[5] = b.hi2 - lo2 * (1 << U);
     }
-    const int u0 = __reduce_min_sync(kFull, b.lo0), u1 = __reduce_min_sync(kFull, b.lo1),
-              u2 = __reduce_min_sync(kFull, b.lo2);
-    const int v0 = __reduce_max_sync(kFull, b.hi0), v1 = __reduce_max_sync(kFull, b.hi1),
-              v2 = __reduce_max_sync(kFull, b.hi2);
+    const int u0 = __reduce_min_sync(kFull, b.lo0) >> U, u1 = __reduce_min_sync(kFull, b.lo1) >> U,
+              u2 = __reduce_min_sync(kFull, b.lo2) >> U;
+    const int v0 = __reduce_max_sync(kFull, b.hi0) >> U, v1 = __reduce_max_sync(kFull, b.hi1) >> U,
+              v2 = __reduce_max_sync(kFull, b.hi2) >> U;
     if (u0 > v0) return __reduce_min_sync(kFull, idt_inactive);  // no active particle takes the tile path
     __syncwarp();
     // every accepted pair lies within 2 max(h_i, largest staged h) of the particle
@@ -1537,19 +1629,22 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
         // sphere that holds every accepted pair
         constexpr float w = kCellWidth;
         constexpr float iw = 1.f / kCellWidth;
+        const float x0 = (float)(x * (1 << U)) * w, x1 = (float)((x + 1) * (1 << U)) * w;
+        const float y0 = (float)(y * (1 << U)) * w, y1 = (float)((y + 1) * (1 << U)) * w;
 #pragma unroll
         for (int k = 0; k < kTileGpw; ++k) {
-            const int bl0 = __shfl_sync(kFull, b.lo0, k * L), bh0 = __shfl_sync(kFull, b.hi0, k * L);
-            const int bl1 = __shfl_sync(kFull, b.lo1, k * L), bh1 = __shfl_sync(kFull, b.hi1, k * L);
-            const int bl2 = __shfl_sync(kFull, b.lo2, k * L), bh2 = __shfl_sync(kFull, b.hi2, k * L);
+            // group k's box in U-units (empty boxes stay empty: kBig >> U > -kBig >> U)
+            const int bl0 = __shfl_sync(kFull, b.lo0, k * L) >> U, bh0 = __shfl_sync(kFull, b.hi0, k * L) >> U;
+            const int bl1 = __shfl_sync(kFull, b.lo1, k * L) >> U, bh1 = __shfl_sync(kFull, b.hi1, k * L) >> U;
+            const int bl2 = __shfl_sync(kFull, b.lo2, k * L) >> U, bh2 = __shfl_sync(kFull, b.hi2, k * L) >> U;
             if (r < rows && x >= bl0 && x <= bh0 && y >= bl1 && y <= bh1) {
-                const float gx = fmaxf(fmaxf((float)x * w - qx[k], qx[k] - (float)(x + 1) * w) - kCellMargin, 0.f);
-                const float gy = fmaxf(fmaxf((float)y * w - qy[k], qy[k] - (float)(y + 1) * w) - kCellMargin, 0.f);
+                const float gx = fmaxf(fmaxf(x0 - qx[k], qx[k] - x1) - kCellMargin, 0.f);
+                const float gy = fmaxf(fmaxf(y0 - qy[k], qy[k] - y1) - kCellMargin, 0.f);
                 const float g2 = gx * gx + gy * gy;
                 if (g2 <= qR[k]) {
                     const float dz = sqrtf(qR[k] - g2);
-                    zl = min(zl, max(bl2, (int)floorf((qz[k] - dz) * iw - 1e-3f)));
-                    zh = max(zh, min(bh2, (int)floorf((qz[k] + dz) * iw + 1e-3f)));
+                    zl = min(zl, max(bl2, (int)floorf((qz[k] - dz) * iw - 1e-3f) >> U));
+                    zh = max(zh, min(bh2, (int)floorf((qz[k] + dz) * iw + 1e-3f) >> U));
                 }
             }
         }
@@ -1635,9 +1730,12 @@ __device__ __forceinline__ int accel_tile_warp(const AccelArgs &a, TileAccShared
     return __reduce_min_sync(kFull, idt);
 }
 
-template <bool KAHAN>
+// The acceleration tile pass U over `tiles` (ctr[0] of them, ctr[1] the
+// ticket), as k_density_tile; deferred particles are counted in *dctr.
+template <bool KAHAN, int U>
 __global__ void __launch_bounds__(kTileThreads, 2)
-    k_acceleration_tile(AccelArgs a, const uint2 *__restrict__ tiles, uint32_t *ctr, uint32_t *__restrict__ deferred) {
+    k_acceleration_tile(AccelArgs a, const uint2 *__restrict__ tiles, uint32_t *ctr, uint32_t *__restrict__ deferred,
+                        uint32_t *dctr) {
     extern __shared__ float4 s_tile_raw[];
     TileAccShared &S = *reinterpret_cast<TileAccShared *>(s_tile_raw);
     const int tid = threadIdx.x, lane = tid & 31;
@@ -1658,21 +1756,26 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         if (S.tile >= ntiles) break;
         const uint32_t tstart = S.start, tend = S.end;
         // a tile whose staged box overflows shared memory is taken again as
-        // its octets, one at a time; an octet that still overflows is handed
-        // to the per-particle pass
-        const bool splittable = (a.skey[tstart] >> 3) != (a.skey[tend - 1] >> 3);
+        // its octets (coarse tiles: its units), one at a time; one that still
+        // overflows is handed to the per-particle pass
+        constexpr int kSplit = U == 0 ? 3 : 3 * U;
+        const bool splittable = (a.skey[tstart] >> kSplit) != (a.skey[tend - 1] >> kSplit);
         bool whole = true;
         uint32_t r0 = tstart;
         while (r0 < tend) {
             __syncthreads();
             if (tid == 0) {
                 uint32_t r1 = tend;
-                if (!whole) {  // the rest of r0's octet
-                    const uint32_t o = a.skey[r0] >> 3;
+                if (!whole) {  // the rest of r0's octet / unit
+                    const uint32_t o = a.skey[r0] >> kSplit;
                     r1 = r0 + 1u;
-                    for (int j = 0; j < 8; ++j) {
-                        const uint2 r = a.cells[o * 8u + (uint32_t)j];
-                        if (r.x != 0xffffffffu) r1 = max(r1, r.y + 1u);
+                    if (U == 0) {
+                        for (int j = 0; j < 8; ++j) {
+                            const uint2 r = a.cells[o * 8u + (uint32_t)j];
+                            if (r.x != 0xffffffffu) r1 = max(r1, r.y + 1u);
+                        }
+                    } else {
+                        r1 = max(r1, a.units[o].y + 1u);
                     }
                 }
                 S.end = r1;
@@ -1690,13 +1793,15 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                     if (!a.active[a.cidx[p]]) continue;
                     const float4 A = a.sA[p];
                     CellBox cb;
-                    if (!accel_box(A.x, A.y, A.z, A.w, cb)) continue;
-                    b[0] = min(b[0], cb.lo0);
-                    b[1] = min(b[1], cb.lo1);
-                    b[2] = min(b[2], cb.lo2);
-                    b[3] = max(b[3], cb.hi0);
-                    b[4] = max(b[4], cb.hi1);
-                    b[5] = max(b[5], cb.hi2);
+                    const int m = accel_mode(A.x, A.y, A.z, A.w, cb, a.coarse);
+                    if (U == 0 && m == kUnitShift) a.cflags[a.skey[p] >> (3 * kUnitShift + 3)] = 1;
+                    if (m != U) continue;
+                    b[0] = min(b[0], cb.lo0 >> U);
+                    b[1] = min(b[1], cb.lo1 >> U);
+                    b[2] = min(b[2], cb.lo2 >> U);
+                    b[3] = max(b[3], cb.hi0 >> U);
+                    b[4] = max(b[4], cb.hi1 >> U);
+                    b[5] = max(b[5], cb.hi2 >> U);
                 }
     #pragma unroll
                 for (int k = 0; k < 3; ++k) {
@@ -1732,7 +1837,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 c_cnt[k] = 0u;
                 if (c < ncell) {
                     const int ix = c / (ny * nz), rem = c - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
-                    const uint2 r = __ldg(a.cells + cell_index_of(lo0 + ix, lo1 + iy, lo2 + iz));
+                    const uint2 r = unit_range<U>(a.cells, a.units, lo0 + ix, lo1 + iy, lo2 + iz);
                     if (r.x != 0xffffffffu) {
                         c_cnt[k] = r.y - r.x + 1u;
                         S.first[c] = r.x;
@@ -1780,7 +1885,21 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                     const float4 q = __ldg(a.sA + gi);
                     S.pos[s] = q;
                     S.gidx[s] = gi;
-                    const int ix = lo / (ny * nz), rem = lo - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
+                    int ix = lo / (ny * nz), rem = lo - ix * ny * nz, iy = rem / nz, iz = rem - iy * nz;
+                    if (U > 0) {
+                        // the particle's cell within its unit: the low 3U bits of its key
+                        const uint32_t key = a.skey[gi];
+                        int dx = 0, dy = 0, dz = 0;
+#pragma unroll
+                        for (int bit = 0; bit < U; ++bit) {
+                            dx |= (int)((key >> (3 * bit)) & 1u) << bit;
+                            dy |= (int)((key >> (3 * bit + 1)) & 1u) << bit;
+                            dz |= (int)((key >> (3 * bit + 2)) & 1u) << bit;
+                        }
+                        ix = (ix << U) | dx;
+                        iy = (iy << U) | dy;
+                        iz = (iz << U) | dz;
+                    }
                     S.scell[s] = (uint32_t)ix | ((uint32_t)iy << 10) | ((uint32_t)iz << 20);
                     hmax = fmaxf(hmax, q.w);
                 }
@@ -1798,7 +1917,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 if (lane == 0) j = atomicAdd(&S.next, (uint32_t)kTileGpw);
                 j = __shfl_sync(0xffffffffu, j, 0);
                 if (start + j >= end) break;
-                wmin = min(wmin, accel_tile_warp<KAHAN>(a, S, start + j, end, lane, tid >> 5, deferred, ctr + 2));
+                wmin = min(wmin, accel_tile_warp<KAHAN, U>(a, S, start + j, end, lane, tid >> 5, deferred, dctr));
             }
             if (lane == 0 && wmin != 0x7fffffff) atomicMin(&S.dtmin, wmin);
             r0 = end;
@@ -1975,10 +2094,16 @@ int tile_smem_opt_in() {
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
     if (!sms[dev]) {
-        cudaFuncSetAttribute(k_density_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileShared));
-        cudaFuncSetAttribute(k_acceleration_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_density_tile<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileShared));
+        cudaFuncSetAttribute(k_density_tile<kUnitShift>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(TileShared));
+        cudaFuncSetAttribute(k_acceleration_tile<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(TileAccShared));
-        cudaFuncSetAttribute(k_acceleration_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_acceleration_tile<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(TileAccShared));
+        cudaFuncSetAttribute(k_acceleration_tile<false, kUnitShift>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(TileAccShared));
+        cudaFuncSetAttribute(k_acceleration_tile<true, kUnitShift>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(TileAccShared));
         int v = 0;
         cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
@@ -2007,6 +2132,9 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     a.cidx = cidx;
     a.skey = ctx->cell_sort.keys[ctx->cell_final];
     a.cells = ctx->cell_range;
+    a.units = ctx->units;
+    a.cflags = ctx->coarse_flags;
+    a.coarse = ctx->tile_coarse;
     a.sp4 = ctx->sp4;
     a.sv4 = ctx->sv4;
     a.h = ctx->h;
@@ -2044,15 +2172,23 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     // one lane per particle, in the reference's order
     k_density<kLanesPerParticle><<<(unsigned)((n + parts - 1) / parts), parts * kLanesPerParticle, smem, st>>>(a);
 #else
+    // cell tiles, then the coarse tiles of the blocks they flagged (the tile
+    // list is reused), then the per-particle pass over what both deferred
     const int sms = tile_smem_opt_in();
-    cudaMemsetAsync(ctx->tile_ctr, 0, sizeof(uint32_t) * 4, st);
-    k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->cell_sort.keys[ctx->cell_final], ctx->cell_range,
-                                                   ctx->tiles, ctx->tile_ctr, ctx->globals, ctx->tile_block_max,
-                                                   ctx->tile_half_max, ctx->tile_big_max);
+    uint32_t *ctr = ctx->tile_ctr;
+    cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * 8, st);
+    k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, a.skey, ctx->cell_range, ctx->tiles, ctr, ctx->globals,
+                                                   ctx->tile_block_max, ctx->tile_half_max, ctx->tile_big_max);
     const unsigned tgrid = tile_grid(n, sms);
-    k_density_tile<<<tgrid, kTileThreads, sizeof(TileShared), st>>>(a, ctx->tiles, ctx->tile_ctr, ctx->deferred);
+    k_density_tile<0><<<tgrid, kTileThreads, sizeof(TileShared), st>>>(a, ctx->tiles, ctr, ctx->deferred, ctr + 2);
+    if (a.coarse) {
+        k_coarse_starts<<<(n + 255) / 256, 256, 0, st>>>(n, a.skey, ctx->units, ctx->coarse_flags, ctx->tiles,
+                                                         ctr + 4);
+        k_density_tile<kUnitShift>
+            <<<tgrid, kTileThreads, sizeof(TileShared), st>>>(a, ctx->tiles, ctr + 4, ctx->deferred, ctr + 2);
+    }
     k_density_deferred<kLanesPerParticle><<<tgrid * 4, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred,
-                                                                                           ctx->tile_ctr + 2);
+                                                                                           ctr + 2);
 #endif
     if (ctx->hs.capture) s = launch_hseed_targets(ctx, st);
     if (s != SPH_OK) return s;
@@ -2067,6 +2203,9 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
     a.cidx = ctx->cell_sort.vals[ctx->cell_final];
     a.skey = ctx->cell_sort.keys[ctx->cell_final];
     a.cells = ctx->cell_range;
+    a.units = ctx->units;
+    a.cflags = ctx->coarse_flags;
+    a.coarse = ctx->tile_coarse;
     a.sA = ctx->sA;
     a.sB = ctx->sB;
     a.sC = ctx->sC;
@@ -2089,24 +2228,34 @@ sph_status launch_acceleration(sph_ctx *ctx, cudaStream_t st) {
         k_acceleration<kLanesPerParticle, false><<<blocks, parts * kLanesPerParticle, smem, st>>>(a);
 #else
     // the density pass's tiles, rebuilt so the pass also stands alone; its own
-    // counters (tile_ctr[4..7])
+    // counters (tile_ctr[8..15]); then the coarse tiles and the deferred
     const int sms = tile_smem_opt_in();
-    uint32_t *ctr = ctx->tile_ctr + 4;
-    cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * 4, st);
-    k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->cell_sort.keys[ctx->cell_final], ctx->cell_range,
-                                                   ctx->tiles, ctr, nullptr, ctx->tile_block_max, ctx->tile_half_max,
-                                                   ctx->tile_big_max);
-    if (kahan) {
-        k_acceleration_tile<true><<<tile_grid(n, sms), kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
-                                                                                         ctx->deferred);
-        k_acceleration_deferred<kLanesPerParticle, true>
-            <<<tile_grid(n, sms) * 4, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
-    } else {
-        k_acceleration_tile<false><<<tile_grid(n, sms), kTileThreads, sizeof(TileAccShared), st>>>(a, ctx->tiles, ctr,
-                                                                                          ctx->deferred);
-        k_acceleration_deferred<kLanesPerParticle, false>
-            <<<tile_grid(n, sms) * 4, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
+    uint32_t *ctr = ctx->tile_ctr + 8;
+    cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * 8, st);
+    k_tile_starts<<<(n + 255) / 256, 256, 0, st>>>(n, a.skey, ctx->cell_range, ctx->tiles, ctr, nullptr,
+                                                   ctx->tile_block_max, ctx->tile_half_max, ctx->tile_big_max);
+    const unsigned tgrid = tile_grid(n, sms);
+    const size_t tsm = sizeof(TileAccShared);
+    if (kahan)
+        k_acceleration_tile<true, 0><<<tgrid, kTileThreads, tsm, st>>>(a, ctx->tiles, ctr, ctx->deferred, ctr + 2);
+    else
+        k_acceleration_tile<false, 0><<<tgrid, kTileThreads, tsm, st>>>(a, ctx->tiles, ctr, ctx->deferred, ctr + 2);
+    if (a.coarse) {
+        k_coarse_starts<<<(n + 255) / 256, 256, 0, st>>>(n, a.skey, ctx->units, ctx->coarse_flags, ctx->tiles,
+                                                         ctr + 4);
+        if (kahan)
+            k_acceleration_tile<true, kUnitShift>
+                <<<tgrid, kTileThreads, tsm, st>>>(a, ctx->tiles, ctr + 4, ctx->deferred, ctr + 2);
+        else
+            k_acceleration_tile<false, kUnitShift>
+                <<<tgrid, kTileThreads, tsm, st>>>(a, ctx->tiles, ctr + 4, ctx->deferred, ctr + 2);
     }
+    if (kahan)
+        k_acceleration_deferred<kLanesPerParticle, true>
+            <<<tgrid * 4, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
+    else
+        k_acceleration_deferred<kLanesPerParticle, false>
+            <<<tgrid * 4, parts * kLanesPerParticle, smem, st>>>(a, ctx->deferred, ctr + 2);
 #endif
     return cuda_status(cudaGetLastError(), "acceleration");
 }

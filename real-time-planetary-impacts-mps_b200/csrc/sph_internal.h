@@ -154,8 +154,9 @@ struct sph_ctx {
     float4 *sp4 = nullptr, *sv4 = nullptr, *sA = nullptr, *sB = nullptr, *sC = nullptr;
     // density and acceleration over cell tiles: (first, end) sorted range of
     // each tile; counters [0] tiles, [1] tile ticket, [2] deferred, [3] spare
-    // for the density pass, [4..7] the same for the acceleration pass; the
-    // sorted indices handed to the per-particle pass
+    // of the density pass's cell tiles, [4] tiles and [5] ticket of its coarse
+    // tiles, [8..13] the same for the acceleration pass; the sorted indices
+    // handed to the per-particle pass
     uint2 *tiles = nullptr;
     uint32_t *tile_ctr = nullptr;
     uint32_t *deferred = nullptr;
@@ -166,6 +167,15 @@ struct sph_ctx {
     uint32_t tile_big_max = 0;
     uint32_t tile_block_max = 320;
     uint32_t tile_half_max = 256;
+    // coarse tiles, for particles whose boxes reach past the cell tiles'
+    // limit: 64-cell units (4 x 4 x 4 cells, indexed by the cell key >> 6)
+    // with their (first, last) sorted index, rebuilt by every sort; a flag per
+    // 512-cell block that holds such a particle, set by the cell-tile passes
+    // and cleared when the coarse tiles are listed.  tile_coarse 0 hands
+    // those particles to the per-particle pass instead.
+    uint2 *units = nullptr;
+    uint8_t *coarse_flags = nullptr;
+    int tile_coarse = 1;
     float2 *eos_forsterite = nullptr, *eos_fe = nullptr;
     sph::EosTables eos{};
 

@@ -175,6 +175,16 @@ __global__ void k_cells(const uint32_t *__restrict__ keys, int n, uint2 *__restr
     if (i == n - 1 || keys[i + 1] != k) cell_range[k].y = (uint32_t)i;
 }
 
+// The unit table: (first, last) sorted index of every occupied 64-cell unit
+// (cell key >> 6); the table is cleared to 0xff bytes before.
+__global__ void k_units(const uint32_t *__restrict__ keys, int n, uint2 *__restrict__ units) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t u = keys[i] >> (3 * kUnitShift);
+    if (i == 0 || (keys[i - 1] >> (3 * kUnitShift)) != u) units[u].x = (uint32_t)i;
+    if (i == n - 1 || (keys[i + 1] >> (3 * kUnitShift)) != u) units[u].y = (uint32_t)i;
+}
+
 __global__ void k_init_cells(uint2 *cell_range, uint32_t count) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
         cell_range[i] = make_uint2(0xffffffffu, 0u);
@@ -351,6 +361,10 @@ sph_status launch_sort(sph_ctx *ctx, cudaStream_t st) {
     ctx->cell_final = fin;
     k_cells<<<(n + 255) / 256, 256, 0, st>>>(s.keys[fin], n, ctx->cell_range);
     ctx->cells_have_prev = true;
+    if (ctx->units) {
+        cudaMemsetAsync(ctx->units, 0xff, sizeof(uint2) * kNumUnits, st);
+        k_units<<<(n + 255) / 256, 256, 0, st>>>(s.keys[fin], n, ctx->units);
+    }
     return cuda_status(cudaGetLastError(), "sort");
 }
 
