@@ -42,6 +42,7 @@ typedef enum {
 #define SPH_HEALTH_SCAN_TIMEOUT      0x0010u /* a scan look-back wait gave up */
 #define SPH_HEALTH_ROOT_LEAF         0x0020u /* the root is a leaf: gravity pass skipped */
 #define SPH_HEALTH_MLP_TIMEOUT       0x0040u /* a tensor-core wait of the h-seed network gave up */
+#define SPH_HEALTH_BAD_INPUT         0x0080u /* sph_step_host received an h outside (0, 10] */
 
 typedef struct sph_ctx sph_ctx;
 
@@ -327,6 +328,32 @@ sph_status sph_selftest_tree_capacity(sph_ctx *ctx, void *stream);
 /* n_steps x (tree, sort, gravity, density, acceleration, step), replayed from
  * a CUDA graph captured on first use (Headless::step without the snapshot). */
 sph_status sph_step_all(sph_ctx *ctx, void *stream, int32_t n_steps);
+
+/* One full step whose state travels through host memory (no counterpart in
+ * the reference, whose Headless loop keeps the state on the device): the
+ * non-NULL fields of `in` are copied to the device at the start of the step
+ * and the non-NULL fields of `out` back at its end, all on `stream` and
+ * asynchronous to the host.  Layouts are sph_upload's: x y z per particle for
+ * the vector fields; pos64 (FP64 positions) in the mixed-precision form and
+ * pos (float positions, the mass kept) in the others.  Every buffer must be
+ * page-locked (cudaHostAlloc, cudaHostRegister) and stay valid until the
+ * stream passes the step.  The positions are copied first; velocity, u, h
+ * and rho are copied on a second stream while the tree, sort and gravity
+ * passes run, and joined before the density pass.  An h outside (0, 10] is
+ * replaced by MAX_SMOOTHING_LENGTH (1) and raises SPH_HEALTH_BAD_INPUT
+ * (sph_synchronize then returns SPH_ERR_DEVICE_HEALTH) rather than being
+ * checked on the host.  The
+ * first call with a set of buffers runs eagerly and waits, then captures a
+ * CUDA graph that later calls with the same buffers replay. */
+typedef struct {
+    double *pos64;
+    float *pos;
+    float *vel;
+    float *u;
+    float *h;
+    float *rho;
+} sph_host_state;
+sph_status sph_step_host(sph_ctx *ctx, const sph_host_state *in, const sph_host_state *out, void *stream);
 
 /* Compute::drawSnapshot (Compute.cpp:396-448, render.metal:49-66): splat the
  * material ids into a 1024x1024 int image by atomic max.  When image is not

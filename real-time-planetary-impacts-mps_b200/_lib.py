@@ -76,6 +76,11 @@ class SphForm(C.Structure):
                 ("h_tolerance", C.c_float), ("timestep", C.c_int32)]
 
 
+class SphHostState(C.Structure):
+    _fields_ = [("pos64", C.c_void_p), ("pos", C.c_void_p), ("vel", C.c_void_p), ("u", C.c_void_p),
+                ("h", C.c_void_p), ("rho", C.c_void_p)]
+
+
 class SphTiling(C.Structure):
     _fields_ = [("big_max", C.c_uint32), ("block_max", C.c_uint32), ("half_max", C.c_uint32), ("coarse", C.c_int32)]
 
@@ -185,6 +190,7 @@ def load(parity: bool = False) -> C.CDLL:
         "sph_acceleration": (st, [vp, vp]),
         "sph_step": (st, [vp, vp]),
         "sph_step_all": (st, [vp, vp, C.c_int32]),
+        "sph_step_host": (st, [vp, C.POINTER(SphHostState), C.POINTER(SphHostState), vp]),
         "sph_sort_cells_noalloc": (st, [vp, C.c_int32, vp, vp, vp]),
         "sph_sort_cells_noalloc_health": (st, [vp, C.POINTER(C.c_uint32)]),
         "sph_selftest_lookback_timeout": (st, [vp, C.c_int32, vp]),

@@ -405,6 +405,34 @@ class Compute:
         self._check(self._lib.sph_download_async(self._h, _lib.FIELDS[field], out.ctypes.data_as(C.c_void_p),
                                                 out.size, _stream(stream)), f"sph_download_async({field})")
 
+    # the layout each field of step_host takes: (elements per particle, dtype)
+    _HOST_STATE = {"pos64": (3, np.float64), "pos": (3, np.float32), "vel": (3, np.float32), "u": (1, np.float32),
+                   "h": (1, np.float32), "rho": (1, np.float32)}
+
+    def step_host(self, inputs: dict, outputs: dict, stream=None) -> None:
+        """One full step with the state moving through host memory
+        (sph_step_host): the arrays of `inputs` are copied in at its start and
+        those of `outputs` filled at its end, asynchronously on `stream`.
+        Fields: pos64 (mixed-precision form) or pos, vel, u, h, rho, in
+        sph_upload's layouts; the arrays must be page-locked (e.g. numpy views
+        of pinned torch tensors) and stay alive until the stream passes the
+        step.  The first call with a set of arrays runs eagerly and captures
+        a graph that later calls with the same arrays replay."""
+        structs = []
+        for d in (inputs, outputs):
+            hs = _lib.SphHostState()
+            for name, a in d.items():
+                if name not in self._HOST_STATE:
+                    raise KeyError(f"step_host: unknown field {name!r}")
+                per, dt = self._HOST_STATE[name]
+                want = per * self.nParticles
+                if a.dtype != dt or not a.flags.c_contiguous or a.size != want:
+                    raise ValueError(f"step_host: {name} needs {want} contiguous {np.dtype(dt).name}")
+                setattr(hs, name, a.ctypes.data)
+            structs.append(hs)
+        self._check(self._lib.sph_step_host(self._h, C.byref(structs[0]), C.byref(structs[1]), _stream(stream)),
+                    "sph_step_host")
+
     def device_buffer(self, field: str):
         """(device pointer, bytes, stride) of a field's storage."""
         p, b, s = C.c_void_p(), C.c_size_t(), C.c_size_t()

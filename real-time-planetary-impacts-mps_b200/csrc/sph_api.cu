@@ -300,8 +300,11 @@ int32_t sph_num_particles(const sph_ctx *ctx) { return ctx ? ctx->n : 0; }
 sph_status sph_destroy(sph_ctx *ctx) {
     if (!ctx) return SPH_OK;
     cudaSetDevice(ctx->device);
-    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+    drop_graphs(ctx);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     void *bufs[] = {ctx->pos4, ctx->vel4, ctx->acc4, ctx->rho, ctx->u, ctx->P, ctx->h, ctx->f, ctx->c,
                     ctx->du, ctx->B, ctx->dhdt, ctx->gnorm, ctx->phi, ctx->mat, ctx->nat, ctx->active, ctx->globals,
                     ctx->health, ctx->cell_range, ctx->sp4, ctx->sv4, ctx->sA, ctx->sB, ctx->sC,
@@ -765,10 +768,7 @@ sph_status sph_set_tree(sph_ctx *ctx, const int32_t *tree, int32_t tree_len, con
         max_branches = std::max<int64_t>(max_branches, br);
     }
     Tree &t = ctx->tree;
-    if (ctx->graph) {
-        cudaGraphExecDestroy(ctx->graph);
-        ctx->graph = nullptr;
-    }
+    drop_graphs(ctx);
     if (n_nodes > t.node_cap || tree_len > t.tree_cap || n_levels > t.max_levels || max_level > t.level_cap ||
         max_branches > t.branch_cap) {
         sph_status s = tree_storage_alloc(
@@ -929,10 +929,7 @@ sph_status sph_set_form(sph_ctx *ctx, const sph_form *f) {
         return SPH_ERR_UNSUPPORTED;
     }
     cudaSetDevice(ctx->device);
-    if (ctx->graph) {
-        cudaGraphExecDestroy(ctx->graph);
-        ctx->graph = nullptr;
-    }
+    drop_graphs(ctx);
     const bool enter_mixed = f->precision == SPH_PRECISION_MIXED && ctx->form.precision != SPH_PRECISION_MIXED;
     ctx->form = *f;
     if (enter_mixed) {
@@ -966,10 +963,7 @@ sph_status sph_set_tiling(sph_ctx *ctx, const sph_tiling *t) {
         return SPH_ERR_INVALID_ARG;
     }
     cudaSetDevice(ctx->device);
-    if (ctx->graph) {
-        cudaGraphExecDestroy(ctx->graph);
-        ctx->graph = nullptr;
-    }
+    drop_graphs(ctx);
     ctx->tile_big_max = t->big_max;
     ctx->tile_block_max = t->block_max;
     ctx->tile_half_max = t->half_max;
@@ -1085,6 +1079,101 @@ sph_status full_step(sph_ctx *ctx, cudaStream_t st) {
     return s;
 }
 
+void drop_graphs(sph_ctx *ctx) {
+    if (ctx->graph) {
+        cudaGraphExecDestroy(ctx->graph);
+        ctx->graph = nullptr;
+    }
+    if (ctx->host_graph) {
+        cudaGraphExecDestroy(ctx->host_graph);
+        ctx->host_graph = nullptr;
+    }
+}
+
+namespace {
+
+// sph_step_host's check of the copied smoothing lengths (sph_upload checks
+// them on the host): an h outside (0, kMaxInitialH] -- whose first density
+// sweep would scan a box wider than the periodic grid -- becomes
+// MAX_SMOOTHING_LENGTH (kMaxH, where the density iteration caps h) and raises
+// SPH_HEALTH_BAD_INPUT.
+__global__ void k_check_h(float *__restrict__ h, int n, uint32_t *health) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = h[i];
+    if (!(v > 0.f) || !(v <= kMaxInitialH)) {
+        h[i] = kMaxH;
+        atomicOr(health, SPH_HEALTH_BAD_INPUT);
+    }
+}
+
+// The step of sph_step_host on st, eager or under capture: the positions'
+// copy, the other inputs' copies on the side stream (joined before the
+// density pass), the passes, then the outputs' copies.  sv4, the sorted
+// velocities, is scratch outside the density pass and stages the velocity
+// copies; ctx->stage stages the positions'.
+sph_status host_step(sph_ctx *ctx, const sph_host_state &in, const sph_host_state &out, cudaStream_t st) {
+    const int n = ctx->n;
+    const size_t n3 = 3 * (size_t)n;
+    const int blocks = (n + 255) / 256;
+    const bool mixed = ctx->form.precision == SPH_PRECISION_MIXED;
+    cudaStream_t sd = ctx->side_stream;
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+    };
+    if (mixed && in.pos64) {
+        ok(cudaMemcpyAsync(ctx->stage, in.pos64, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
+        k_pack3d<<<blocks, 256, 0, st>>>((const double *)ctx->stage, ctx->pos64, ctx->pos4, n);
+    } else if (!mixed && in.pos) {
+        ok(cudaMemcpyAsync(ctx->stage, in.pos, sizeof(float) * n3, cudaMemcpyHostToDevice, st));
+        k_pack3<<<blocks, 256, 0, st>>>((const float *)ctx->stage, ctx->pos4, n, 1);
+    }
+    ok(cudaEventRecord(ctx->ev_fork, st));
+    ok(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
+    if (in.vel) {
+        ok(cudaMemcpyAsync(ctx->sv4, in.vel, sizeof(float) * n3, cudaMemcpyHostToDevice, sd));
+        k_pack3<<<blocks, 256, 0, sd>>>((const float *)ctx->sv4, ctx->vel4, n, 0);
+    }
+    if (in.u) ok(cudaMemcpyAsync(ctx->u, in.u, sizeof(float) * n, cudaMemcpyHostToDevice, sd));
+    if (in.h) {
+        ok(cudaMemcpyAsync(ctx->h, in.h, sizeof(float) * n, cudaMemcpyHostToDevice, sd));
+        k_check_h<<<blocks, 256, 0, sd>>>(ctx->h, n, ctx->health);
+    }
+    if (in.rho) ok(cudaMemcpyAsync(ctx->rho, in.rho, sizeof(float) * n, cudaMemcpyHostToDevice, sd));
+    ok(cudaEventRecord(ctx->ev_join, sd));
+    ok(cudaGetLastError());
+    sph_status s = e == cudaSuccess ? SPH_OK : cuda_status(e, "sph_step_host inputs");
+    if (s == SPH_OK && ctx->params.tree_source == SPH_TREE_GPU) s = launch_tree_build(ctx, st);
+    if (s == SPH_OK) s = launch_sort(ctx, st);
+    if (s == SPH_OK) s = gravity_pass(ctx, st);
+    // joined whatever happened, so that a capture ends well formed
+    cudaError_t ej = cudaStreamWaitEvent(st, ctx->ev_join, 0);
+    if (s == SPH_OK && ej != cudaSuccess) s = cuda_status(ej, "sph_step_host join");
+    if (s == SPH_OK) s = launch_density(ctx, st);
+    if (s == SPH_OK) s = launch_acceleration(ctx, st);
+    if (s == SPH_OK) s = launch_step(ctx, st);
+    if (s != SPH_OK) return s;
+    if (mixed && out.pos64) {
+        k_unpack3d<<<blocks, 256, 0, st>>>(ctx->pos64, (double *)ctx->stage, n);
+        ok(cudaMemcpyAsync(out.pos64, ctx->stage, sizeof(double) * n3, cudaMemcpyDeviceToHost, st));
+    } else if (!mixed && out.pos) {
+        k_unpack3<<<blocks, 256, 0, st>>>(ctx->pos4, (float *)ctx->stage, n);
+        ok(cudaMemcpyAsync(out.pos, ctx->stage, sizeof(float) * n3, cudaMemcpyDeviceToHost, st));
+    }
+    if (out.vel) {
+        k_unpack3<<<blocks, 256, 0, st>>>(ctx->vel4, (float *)ctx->sv4, n);
+        ok(cudaMemcpyAsync(out.vel, ctx->sv4, sizeof(float) * n3, cudaMemcpyDeviceToHost, st));
+    }
+    if (out.u) ok(cudaMemcpyAsync(out.u, ctx->u, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    if (out.h) ok(cudaMemcpyAsync(out.h, ctx->h, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    if (out.rho) ok(cudaMemcpyAsync(out.rho, ctx->rho, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    ok(cudaGetLastError());
+    return cuda_status(e, "sph_step_host outputs");
+}
+
+}  // namespace
+
 }  // namespace sph
 
 extern "C" {
@@ -1123,6 +1212,66 @@ sph_status sph_step_all(sph_ctx *ctx, void *stream, int32_t n_steps) {
         cudaError_t e = cudaGraphLaunch(ctx->graph, st);
         if (e != cudaSuccess) return cuda_status(e, "graph launch");
     }
+    return SPH_OK;
+}
+
+sph_status sph_step_host(sph_ctx *ctx, const sph_host_state *in, const sph_host_state *out, void *stream) {
+    if (!ctx || !in || !out) return SPH_ERR_INVALID_ARG;
+    const bool mixed = ctx->form.precision == SPH_PRECISION_MIXED;
+    if (mixed ? (in->pos || out->pos) : (in->pos64 || out->pos64)) {
+        set_error("sph_step_host: %s", mixed ? "the mixed-precision form moves FP64 positions (pos64), not pos"
+                                             : "FP64 positions (pos64) exist in the mixed-precision form only");
+        return SPH_ERR_INVALID_ARG;
+    }
+    const void *bufs[] = {in->pos64, in->pos, in->vel, in->u, in->h, in->rho,
+                          out->pos64, out->pos, out->vel, out->u, out->h, out->rho};
+    for (const void *b : bufs) {
+        if (!b) continue;
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, b) != cudaSuccess || at.type != cudaMemoryTypeHost) {
+            cudaGetLastError();
+            set_error("sph_step_host: host buffers must be page-locked (cudaHostAlloc / cudaHostRegister)");
+            return SPH_ERR_INVALID_ARG;
+        }
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (!ctx->own_stream) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ctx->side_stream) e = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ctx->ev_fork) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess && !ctx->ev_join) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_status(e, "sph_step_host streams");
+    const bool same = ctx->host_graph && std::memcmp(&ctx->host_in, in, sizeof(*in)) == 0 &&
+                      std::memcmp(&ctx->host_out, out, sizeof(*out)) == 0;
+    if (same) return cuda_status(cudaGraphLaunch(ctx->host_graph, st), "sph_step_host graph launch");
+    if (ctx->host_graph) {
+        cudaGraphExecDestroy(ctx->host_graph);
+        ctx->host_graph = nullptr;
+    }
+    // this call's step runs eagerly (it also settles the sort's buffer roles);
+    // the graph for the next calls is captured after it
+    sph_status s = host_step(ctx, *in, *out, st);
+    if (s != SPH_OK) return s;
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e, "sph_step_host eager step");
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_status(e, "sph_step_host begin capture");
+    s = host_step(ctx, *in, *out, ctx->own_stream);
+    e = cudaStreamEndCapture(ctx->own_stream, &g);
+    if (s != SPH_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return s != SPH_OK ? s : cuda_status(e, "sph_step_host end capture");
+    }
+    e = cudaGraphInstantiate(&ctx->host_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        ctx->host_graph = nullptr;
+        return cuda_status(e, "sph_step_host graph instantiate");
+    }
+    ctx->host_in = *in;
+    ctx->host_out = *out;
     return SPH_OK;
 }
 

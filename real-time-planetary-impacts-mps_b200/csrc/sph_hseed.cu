@@ -544,10 +544,7 @@ sph_status sph_hseed_capture(sph_ctx *ctx, int32_t on) {
         sph_status s = hseed_alloc(ctx);
         if (s != SPH_OK) return s;
     }
-    if (ctx->graph) {
-        cudaGraphExecDestroy(ctx->graph);
-        ctx->graph = nullptr;
-    }
+    drop_graphs(ctx);
     ctx->hs.capture = on != 0;
     return SPH_OK;
 }

@@ -604,6 +604,7 @@ struct TileShared {
     uint32_t start, end, tile, next;
     uint32_t stats[4];
     int defer_all;
+    int need;                           // some particle of the range needs the warp pass
 };
 
 // The list box of a tile particle at smoothing length hb: the cells within
@@ -1130,15 +1131,22 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 S.box[0] = S.box[1] = S.box[2] = 0x7fffffff;
                 S.box[3] = S.box[4] = S.box[5] = -0x7fffffff;
                 S.defer_all = 0;
+                S.need = 0;
             }
             __syncthreads();
             const uint32_t start = r0, end = S.end;
             // the staged box: union of the list boxes of the tile's active particles
             {
                 int b[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, -0x7fffffff, -0x7fffffff, -0x7fffffff};
+                // the warp pass is needed for this pass's particles and, in the
+                // cell-tile pass, for the inactive (EOS only) and deferred ones
+                bool need = false;
                 for (uint32_t p = start + tid; p < end; p += kTileThreads) {
                     const uint32_t ind = a.cidx[p];
-                    if (!a.active[ind]) continue;
+                    if (!a.active[ind]) {
+                        need |= U == 0;
+                        continue;
+                    }
                     const float4 me = a.sp4[p];
                     const float h_plain = a.h[ind];
                     bool seeded;
@@ -1146,6 +1154,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                     const float hb = fmaxf(h0, h_plain);
                     const int m = density_mode(me.x, me.y, me.z, hb, a.coarse);
                     if (U == 0 && m == kUnitShift) a.cflags[a.skey[p] >> (3 * kUnitShift + 3)] = 1;
+                    need |= m == U || (U == 0 && m < 0);
                     if (m != U) continue;
                     CellBox cb;
                     tile_box(me.x, me.y, me.z, hb, cb, fmaxf(kTileStageReach, kTileListReach));
@@ -1161,6 +1170,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                     b[k] = __reduce_min_sync(0xffffffffu, b[k]);
                     b[k + 3] = __reduce_max_sync(0xffffffffu, b[k + 3]);
                 }
+                if (__any_sync(0xffffffffu, need) && lane == 0) S.need = 1;
                 if (lane == 0) {
     #pragma unroll
                     for (int k = 0; k < 3; ++k) {
@@ -1241,12 +1251,14 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 }
             }
             __syncthreads();
-            // warps take the tile's particles four at a time
-            for (;;) {
+            // warps take the tile's particles four at a time (none when no
+            // particle of the range needs this pass)
+            for (bool more = S.need != 0; more;) {
                 uint32_t j = 0u;
                 if (lane == 0) j = atomicAdd(&S.next, (uint32_t)kTileGpw);
                 j = __shfl_sync(0xffffffffu, j, 0);
-                if (start + j >= end) break;
+                more = start + j < end;
+                if (!more) break;
                 density_tile_warp<U>(a, S, S.stats, start + j, end, lane, &S.list[(tid >> 5) * kTileGpw], deferred,
                                      dctr);
             }
@@ -1518,6 +1530,7 @@ struct TileAccShared {
     uint32_t wsum[kTileThreads / 32];
     uint32_t start, end, tile, next;
     int defer_all;
+    int need;                           // some particle of the range needs the warp pass
     int dtmin;
     int hmax_bits;                      // largest staged h (float bits; h > 0)
 };
@@ -1783,18 +1796,27 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 S.box[0] = S.box[1] = S.box[2] = 0x7fffffff;
                 S.box[3] = S.box[4] = S.box[5] = -0x7fffffff;
                 S.defer_all = 0;
+                S.need = 0;
                 S.hmax_bits = 0;
             }
             __syncthreads();
             const uint32_t start = r0, end = S.end;
             {
                 int b[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, -0x7fffffff, -0x7fffffff, -0x7fffffff};
+                // the warp pass is needed for this pass's particles and, in the
+                // cell-tile pass, for the inactive (their next active time bounds
+                // the step) and deferred ones
+                bool need = false;
                 for (uint32_t p = start + tid; p < end; p += kTileThreads) {
-                    if (!a.active[a.cidx[p]]) continue;
+                    if (!a.active[a.cidx[p]]) {
+                        need |= U == 0;
+                        continue;
+                    }
                     const float4 A = a.sA[p];
                     CellBox cb;
                     const int m = accel_mode(A.x, A.y, A.z, A.w, cb, a.coarse);
                     if (U == 0 && m == kUnitShift) a.cflags[a.skey[p] >> (3 * kUnitShift + 3)] = 1;
+                    need |= m == U || (U == 0 && m < 0);
                     if (m != U) continue;
                     b[0] = min(b[0], cb.lo0 >> U);
                     b[1] = min(b[1], cb.lo1 >> U);
@@ -1808,6 +1830,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                     b[k] = __reduce_min_sync(0xffffffffu, b[k]);
                     b[k + 3] = __reduce_max_sync(0xffffffffu, b[k + 3]);
                 }
+                if (__any_sync(0xffffffffu, need) && lane == 0) S.need = 1;
                 if (lane == 0) {
     #pragma unroll
                     for (int k = 0; k < 3; ++k) {
@@ -1912,11 +1935,12 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             }
             __syncthreads();
             int wmin = 0x7fffffff;
-            for (;;) {
+            for (bool more = S.need != 0; more;) {  // none when no particle of the range needs this pass
                 uint32_t j = 0u;
                 if (lane == 0) j = atomicAdd(&S.next, (uint32_t)kTileGpw);
                 j = __shfl_sync(0xffffffffu, j, 0);
-                if (start + j >= end) break;
+                more = start + j < end;
+                if (!more) break;
                 wmin = min(wmin, accel_tile_warp<KAHAN, U>(a, S, start + j, end, lane, tid >> 5, deferred, dctr));
             }
             if (lane == 0 && wmin != 0x7fffffff) atomicMin(&S.dtmin, wmin);

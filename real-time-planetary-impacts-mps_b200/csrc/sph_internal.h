@@ -191,6 +191,12 @@ struct sph_ctx {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     cudaStream_t own_stream = nullptr;
+    // sph_step_host: its graph, the host buffers it was captured for, and the
+    // side stream and events of the overlapped input copies
+    cudaGraphExec_t host_graph = nullptr;
+    sph_host_state host_in{}, host_out{};
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 namespace sph {
@@ -249,6 +255,9 @@ sph_status launch_tree_build(sph_ctx *ctx, cudaStream_t st);
 // sph_api.cu
 // One full step (tree, sort, gravity, density, acceleration, step) on st.
 sph_status full_step(sph_ctx *ctx, cudaStream_t st);
+// Destroy the captured step graphs (sph_step_all's and sph_step_host's):
+// called whenever what they replay changes.
+void drop_graphs(sph_ctx *ctx);
 void set_error(const char *fmt, ...);
 sph_status cuda_status(cudaError_t e, const char *what);
 
