@@ -14,7 +14,9 @@ Forms (one context each, same initial conditions):
           positions, plain initial h guess) -- what the parity tests pin;
   chosen  opening-angle gravity (theta, default 0.6), mixed precision (FP64
           master positions and time, Kahan sums) and the learned h seed,
-          trained online on the first steps' density passes.
+          trained on the warm-up steps' density passes and refreshed every
+          step (--online-iters Adam steps beside the tree, sort and gravity
+          passes, inside the timed steps).
 `value` is the chosen form; `chosen_over_plain` is the ratio of the two
 graph-replayed step times.  The line also carries the gravity error of both
 forms against an FP64 direct sum (16 384 targets), the total-energy drift of
@@ -453,6 +455,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="particle count relative to 1e6 (diagnostics)")
     ap.add_argument("--theta", type=float, default=0.6, help="opening angle of the chosen form's gravity")
     ap.add_argument("--train-iters", type=int, default=600, help="Adam steps after each warm-up step")
+    ap.add_argument("--online-iters", type=int, default=8,
+                    help="Adam steps of the seed's online refresh per step (0: seed trained in warm-up only)")
     ap.add_argument("--drift-steps", type=int, default=100,
                     help="steps of the energy-drift comparison (the 1000-step comparison runs at config 0 in the tests)")
     ap.add_argument("--ensemble", type=int, default=0,
@@ -516,6 +520,8 @@ def main():
             train_ms.append((time.perf_counter() - t0) * 1e3)
     cc.hseed_capture(False)
     cc.set_form(gravity="theta", theta=args.theta, precision="mixed", h_seed="learned")
+    if args.online_iters > 0:
+        cc.hseed_online(args.online_iters, 16384, 1e-3)
     with torch.cuda.stream(stream):
         cc.step(stream)
     stream.synchronize()
@@ -608,7 +614,9 @@ def main():
             "vs_baseline": None, "dtype": "f32 (FP64 positions, time and reductions in the chosen form)",
             "data": "synthetic (seeded two-body impact generator)",
             "config": {"workload": f"two-body impact N={n} (800k+200k), leaf {LEAF}, depth {DEPTH}",
-                       "form": f"chosen: theta {args.theta} gravity + mixed precision + learned h seed",
+                       "form": f"chosen: theta {args.theta} gravity + mixed precision + learned h seed"
+                               + (f" (refreshed online, {args.online_iters} Adam steps per step)"
+                                  if args.online_iters > 0 else ""),
                        "n_particles": n, "leaf_capacity": LEAF, "max_tree_depth": DEPTH,
                        "parallelism": f"replicas x{world}", "l2": "state larger than L2 (no flush)",
                        "timing": mode_c},
@@ -623,7 +631,8 @@ def main():
                        "acceleration_deferred_particles": st["accel_deferred"],
                        "density_coarse_tiles": st["coarse_tiles"],
                        "acceleration_coarse_tiles": st["accel_coarse_tiles"],
-                       "training_ms_per_call": float(np.mean(train_ms)), "adam_steps_per_call": args.train_iters},
+                       "training_ms_per_call": float(np.mean(train_ms)), "adam_steps_per_call": args.train_iters,
+                       "online_adam_steps_per_step": args.online_iters},
             "roofline": {"bound": "hbm", "kernel": f"{dom} pass ({PASS_KERNELS[dom]}), chosen form",
                          "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],

@@ -217,15 +217,16 @@ sph_status sph_gravity_direct_f64(sph_ctx *ctx, const int32_t *targets, int32_t 
 /* Learned smoothing-length seed (no counterpart in the reference).  An
  * 8 -> 64 -> 64 -> 1 MLP, run and trained on the tensor cores (BF16 operands,
  * FP32 accumulation), predicts from a particle's state at the start of the
- * density pass the h its iteration converges to; SPH_HSEED_LEARNED starts the
- * iteration there (density.metal:73-143), falling back to the plain guess
- * when the first sweep moves the seed by more than 5%.
+ * density pass the fixed point its iteration approaches, h_fix =
+ * RESOLUTION_ETA (m / rho)^(1/3) at the converged density; SPH_HSEED_LEARNED
+ * starts the iteration there (density.metal:73-143), falling back to the
+ * plain guess when the first sweep moves the seed by more than 5%.
  * sph_hseed_capture(ctx, 1): every following density pass records its
- *   (features, converged h) pairs as the training set (the last pass's).
+ *   (features, log(h_fix / h0)) pairs as the training set (the last pass's).
  * sph_hseed_train: `iterations` Adam steps (learning rate lr) on minibatches
- *   of `batch` rows drawn from the recorded set; the first call also fixes
- *   the feature and target standardisation.  *loss = the last minibatch's
- *   mean squared error (standardised target), may be NULL.  Synchronous.
+ *   of `batch` rows drawn from the recorded set, after deriving the feature
+ *   and target standardisation from it.  *loss = the last minibatch's mean
+ *   squared error (standardised target), may be NULL.  Synchronous.
  * sph_hseed_gradient: the loss gradient of one minibatch (row r of the batch
  *   is particle ((r * 0x9E3779B97F4A7C15) ^ salt) mod n, arithmetic modulo
  *   2^64) without updating the weights: grads receives
@@ -233,7 +234,7 @@ sph_status sph_gravity_direct_f64(sph_ctx *ctx, const int32_t *targets, int32_t 
  *   W2[64][64], b2[64], w3[64], b3.  Synchronous.
  * sph_hseed_params: copy the FP32 weights out (get) and/or in (set); either
  *   may be NULL.  sph_hseed_dataset: the recorded raw features [n][8],
- *   targets log(h_converged / h0) [n] and the standardisation (feature means
+ *   targets log(h_fix / h0) [n] and the standardisation (feature means
  *   [8], feature 1/deviations [8], target mean, target deviation); any may be
  *   NULL.
  * sph_hseed_stats: counters of the last density pass. */
@@ -253,6 +254,17 @@ int32_t sph_hseed_num_params(void);
 sph_status sph_hseed_capture(sph_ctx *ctx, int32_t on);
 sph_status sph_hseed_train(sph_ctx *ctx, int32_t iterations, int32_t batch, float lr, float *loss, void *stream);
 sph_status sph_hseed_gradient(sph_ctx *ctx, int32_t batch, uint32_t salt, float *grads, float *loss, void *stream);
+/* Online refresh of the learned seed: with iterations > 0, every density pass
+ * records its pairs (as sph_hseed_capture) and, while the learned seed is the
+ * form's start, each step first takes `iterations` Adam steps (minibatch
+ * `batch`, rate lr) on the previous pass's pairs, after re-deriving the
+ * standardisation from them.  In sph_step_all, sph_step_host and ensembles
+ * these steps run on a second stream beside the tree, sort and gravity
+ * passes and are joined before the density pass; in a lone sph_density they
+ * run at its start.  The seed otherwise drifts from the state it was trained
+ * on: its sweeps per particle grow step by step.  iterations = 0 turns the
+ * refresh and the recording off.  Drops a captured step graph. */
+sph_status sph_hseed_online(sph_ctx *ctx, int32_t iterations, int32_t batch, float lr);
 sph_status sph_hseed_params(sph_ctx *ctx, float *get, const float *set);
 sph_status sph_hseed_dataset(sph_ctx *ctx, float *features, float *targets, float *norm);
 /* The seed network's input/target standardisation (18 floats, the layout of

@@ -208,6 +208,7 @@ def load(parity: bool = False) -> C.CDLL:
         "sph_hseed_capture": (st, [vp, C.c_int32]),
         "sph_hseed_train": (st, [vp, C.c_int32, C.c_int32, C.c_float, _fp, vp]),
         "sph_hseed_gradient": (st, [vp, C.c_int32, C.c_uint32, _fp, _fp, vp]),
+        "sph_hseed_online": (st, [vp, C.c_int32, C.c_int32, C.c_float]),
         "sph_hseed_params": (st, [vp, _fp, _fp]),
         "sph_hseed_dataset": (st, [vp, _fp, _fp, _fp]),
         "sph_hseed_norm": (st, [vp, _fp, _fp]),

@@ -281,6 +281,13 @@ class Compute:
                                               _stream(stream)), "sph_hseed_train")
         return loss.value
 
+    def hseed_online(self, iterations: int, batch: int = 16384, lr: float = 1e-3):
+        """Online refresh of the learned seed (sph_hseed_online): every
+        density pass records its pairs and each step first takes `iterations`
+        Adam steps on the previous pass's (beside the tree, sort and gravity
+        passes in graph-replayed steps).  0 turns it off."""
+        self._check(self._lib.sph_hseed_online(self._h, int(iterations), int(batch), float(lr)), "sph_hseed_online")
+
     def hseed_gradient(self, batch: int, salt: int, stream=None):
         """(gradient, loss) of one minibatch, weights unchanged."""
         g = np.zeros(self._lib.sph_hseed_num_params(), np.float32)

@@ -1068,12 +1068,42 @@ sph_status sph_step(sph_ctx *ctx, void *stream) {
 namespace sph {
 
 // One full step (Headless.cpp:43-51 without the snapshot) on `st`.
+// The side stream and the fork / join events of a step (created once).
+sph_status ensure_side(sph_ctx *ctx) {
+    cudaError_t e = cudaSuccess;
+    if (!ctx->side_stream) e = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ctx->ev_fork) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess && !ctx->ev_join) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+    return cuda_status(e, "side stream");
+}
+
 sph_status full_step(sph_ctx *ctx, cudaStream_t st) {
     sph_status s = SPH_OK;
-    if (ctx->params.tree_source == SPH_TREE_GPU) s = launch_tree_build(ctx, st);
+    // the learned seed's online refresh runs beside the tree, sort and
+    // gravity passes (it reads the previous density pass's pairs and writes
+    // only the network) and is joined before the density pass
+    const bool ahead = hseed_online_due(ctx);
+    if (ahead) {
+        s = ensure_side(ctx);
+        cudaError_t e = cudaSuccess;
+        if (s == SPH_OK) e = cudaEventRecord(ctx->ev_fork, st);
+        if (s == SPH_OK && e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0);
+        if (s == SPH_OK && e != cudaSuccess) s = cuda_status(e, "full step fork");
+        if (s == SPH_OK) s = launch_hseed_online(ctx, ctx->side_stream);
+        // recorded whatever happened, so that a capture ends well formed
+        cudaError_t ej = cudaEventRecord(ctx->ev_join, ctx->side_stream);
+        if (s == SPH_OK && ej != cudaSuccess) s = cuda_status(ej, "full step join");
+        ctx->hs.trained_ahead = s == SPH_OK;
+    }
+    if (s == SPH_OK && ctx->params.tree_source == SPH_TREE_GPU) s = launch_tree_build(ctx, st);
     if (s == SPH_OK) s = launch_sort(ctx, st);
     if (s == SPH_OK) s = gravity_pass(ctx, st);
+    if (ahead) {
+        cudaError_t ej = cudaStreamWaitEvent(st, ctx->ev_join, 0);
+        if (s == SPH_OK && ej != cudaSuccess) s = cuda_status(ej, "full step join");
+    }
     if (s == SPH_OK) s = launch_density(ctx, st);
+    ctx->hs.trained_ahead = false;
     if (s == SPH_OK) s = launch_acceleration(ctx, st);
     if (s == SPH_OK) s = launch_step(ctx, st);
     return s;
@@ -1141,9 +1171,14 @@ sph_status host_step(sph_ctx *ctx, const sph_host_state &in, const sph_host_stat
         k_check_h<<<blocks, 256, 0, sd>>>(ctx->h, n, ctx->health);
     }
     if (in.rho) ok(cudaMemcpyAsync(ctx->rho, in.rho, sizeof(float) * n, cudaMemcpyHostToDevice, sd));
-    ok(cudaEventRecord(ctx->ev_join, sd));
     ok(cudaGetLastError());
     sph_status s = e == cudaSuccess ? SPH_OK : cuda_status(e, "sph_step_host inputs");
+    // the learned seed's online refresh follows on the side stream (full_step)
+    if (s == SPH_OK && hseed_online_due(ctx)) {
+        s = launch_hseed_online(ctx, sd);
+        ctx->hs.trained_ahead = s == SPH_OK;
+    }
+    ok(cudaEventRecord(ctx->ev_join, sd));
     if (s == SPH_OK && ctx->params.tree_source == SPH_TREE_GPU) s = launch_tree_build(ctx, st);
     if (s == SPH_OK) s = launch_sort(ctx, st);
     if (s == SPH_OK) s = gravity_pass(ctx, st);
@@ -1151,6 +1186,7 @@ sph_status host_step(sph_ctx *ctx, const sph_host_state &in, const sph_host_stat
     cudaError_t ej = cudaStreamWaitEvent(st, ctx->ev_join, 0);
     if (s == SPH_OK && ej != cudaSuccess) s = cuda_status(ej, "sph_step_host join");
     if (s == SPH_OK) s = launch_density(ctx, st);
+    ctx->hs.trained_ahead = false;
     if (s == SPH_OK) s = launch_acceleration(ctx, st);
     if (s == SPH_OK) s = launch_step(ctx, st);
     if (s != SPH_OK) return s;
@@ -1238,10 +1274,9 @@ sph_status sph_step_host(sph_ctx *ctx, const sph_host_state *in, const sph_host_
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = cudaSuccess;
     if (!ctx->own_stream) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess && !ctx->side_stream) e = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess && !ctx->ev_fork) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
-    if (e == cudaSuccess && !ctx->ev_join) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
-    if (e != cudaSuccess) return cuda_status(e, "sph_step_host streams");
+    if (e != cudaSuccess) return cuda_status(e, "sph_step_host stream");
+    sph_status s = ensure_side(ctx);
+    if (s != SPH_OK) return s;
     const bool same = ctx->host_graph && std::memcmp(&ctx->host_in, in, sizeof(*in)) == 0 &&
                       std::memcmp(&ctx->host_out, out, sizeof(*out)) == 0;
     if (same) return cuda_status(cudaGraphLaunch(ctx->host_graph, st), "sph_step_host graph launch");
@@ -1251,7 +1286,7 @@ sph_status sph_step_host(sph_ctx *ctx, const sph_host_state *in, const sph_host_
     }
     // this call's step runs eagerly (it also settles the sort's buffer roles);
     // the graph for the next calls is captured after it
-    sph_status s = host_step(ctx, *in, *out, st);
+    s = host_step(ctx, *in, *out, st);
     if (s != SPH_OK) return s;
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_status(e, "sph_step_host eager step");

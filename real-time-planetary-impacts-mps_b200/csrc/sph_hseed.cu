@@ -97,11 +97,20 @@ __global__ void k_hs_capture(HSeedArgs a) {
     a.h0[i] = a.h[i];
 }
 
-// Training targets after the pass: log(h_converged / h0).
+// Training targets after the pass: log(h_fix / h0), h_fix = RESOLUTION_ETA
+// (m / rho)^(1/3) (capped at MAX_H) from the converged density -- the fixed
+// point the iteration approaches.  The converged h itself stops within
+// DENSITY_ETA of it on the side the iteration came from, so it depends on
+// the start: trained on it, a seed learns the plain start's lag, and once
+// the seed starts the iteration the next step's h0 carries a different lag
+// than the training pairs did, and the seed drifts off.  The fixed point does
+// not depend on the start, and a seed at it converges in one sweep.
 __global__ void k_hs_targets(HSeedArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
-    a.y[i] = logf(a.h[i] / a.h0[i]);
+    const float m = a.pos4[i].w, rho = fmaxf(a.rho[i], 1e-30f);
+    const float h_fix = fminf(kResolutionEta * cbrtf(m / rho), kMaxH);
+    a.y[i] = logf(h_fix / a.h0[i]);
 }
 
 // FP64 mean and second moment of the features and the target (block partials
@@ -161,8 +170,9 @@ __device__ __forceinline__ int sample_row(uint32_t it, uint32_t row, int batch, 
 
 // MODE 0: inference (features from the state, writes the seed); MODE 1:
 // gradients of the loss 1/2 mean (y - t)^2 over `batch` sampled rows.
+// MODE 1 samples its rows for iteration it + *it_base (it_base may be null).
 template <int MODE>
-__global__ void __launch_bounds__(kTile) k_mlp(HSeedArgs a, uint32_t it, int batch) {
+__global__ void __launch_bounds__(kTile) k_mlp(HSeedArgs a, uint32_t it, int batch, const uint32_t *it_base) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ uint64_t bar;
     __shared__ uint32_t tmem_slot;
@@ -208,7 +218,7 @@ __global__ void __launch_bounds__(kTile) k_mlp(HSeedArgs a, uint32_t it, int bat
     } else {
         valid = (int)(blockIdx.x * kTile + t) < batch;
         if (valid) {
-            row = sample_row(it, blockIdx.x * kTile + t, batch, a.n, a.salt);
+            row = sample_row(it + (it_base ? *it_base : 0u), blockIdx.x * kTile + t, batch, a.n, a.salt);
 #pragma unroll
             for (int k = 0; k < kIn; ++k) x[k] = a.X[(size_t)row * kIn + k];
             target = (a.y[row] - norm[2 * kIn]) / norm[2 * kIn + 1];
@@ -375,20 +385,26 @@ __global__ void __launch_bounds__(kTile) k_mlp(HSeedArgs a, uint32_t it, int bat
     if (warp == 0) tc::tmem_dealloc(tm, tmem_cols<MODE>());
 }
 
-// Adam on the FP32 master weights; clears the gradient.
-__global__ void k_adam(float *params, float *grads, float *m, float *v, int s, float lr) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < kNParams) {
-        const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+// Adam on the FP32 master weights (one CTA); clears the gradient and counts
+// the step in the device counter *step, so that replays of a captured graph
+// keep counting (bias correction, sample rows).
+constexpr int kAdamThreads = 1024;
+__global__ void __launch_bounds__(kAdamThreads) k_adam(float *params, float *grads, float *m, float *v,
+                                                        uint32_t *step, float lr) {
+    const float s = (float)(*step + 1u);
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float c1 = 1.f - powf(b1, s), c2 = 1.f - powf(b2, s);
+    for (int k = threadIdx.x; k < kNParams; k += kAdamThreads) {
         const float g = grads[k];
         const float mk = b1 * m[k] + (1.f - b1) * g;
         const float vk = b2 * v[k] + (1.f - b2) * g * g;
         m[k] = mk;
         v[k] = vk;
-        const float mh = mk / (1.f - powf(b1, (float)s)), vh = vk / (1.f - powf(b2, (float)s));
-        params[k] -= lr * mh / (sqrtf(vh) + eps);
+        params[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
         grads[k] = 0.f;
     }
+    __syncthreads();  // every thread has read *step
+    if (threadIdx.x == 0) *step += 1u;
 }
 
 }  // namespace
@@ -418,6 +434,7 @@ sph_status hseed_alloc(sph_ctx *ctx) {
     chk(cudaMalloc(&hs.seed, sizeof(float) * n));
     chk(cudaMalloc(&hs.loss, sizeof(float)));
     chk(cudaMalloc(&hs.stats, sizeof(uint32_t) * 4));
+    chk(cudaMalloc(&hs.adam_step, sizeof(uint32_t)));
     if (e != cudaSuccess) return cuda_status(e, "learned h seed buffers");
     // He-style initialisation, seeded (the host draws, the device keeps)
     std::vector<float> p(kNParams, 0.f);
@@ -441,6 +458,7 @@ sph_status hseed_alloc(sph_ctx *ctx) {
     chk(cudaMemset(hs.adam_v, 0, sizeof(float) * kNParams));
     chk(cudaMemset(hs.nn, 0, sizeof(float) * n));
     chk(cudaMemset(hs.stats, 0, sizeof(uint32_t) * 4));
+    chk(cudaMemset(hs.adam_step, 0, sizeof(uint32_t)));
     if (e == cudaSuccess) {
         static bool attr = false;
         if (!attr) {
@@ -454,8 +472,8 @@ sph_status hseed_alloc(sph_ctx *ctx) {
 
 void hseed_free(sph_ctx *ctx) {
     HSeed &hs = ctx->hs;
-    void *bufs[] = {hs.params, hs.grads, hs.adam_m, hs.adam_v, hs.norm, hs.norm_part, hs.X,
-                    hs.y,      hs.h0,    hs.nn,     hs.seed,   hs.loss,  hs.stats};
+    void *bufs[] = {hs.params, hs.grads, hs.adam_m, hs.adam_v, hs.norm,  hs.norm_part, hs.X,
+                    hs.y,      hs.h0,    hs.nn,     hs.seed,   hs.loss, hs.stats,     hs.adam_step};
     for (void *b : bufs) cudaFree(b);
     hs = HSeed();
 }
@@ -464,6 +482,7 @@ HSeedArgs hseed_args(sph_ctx *ctx) {
     HSeed &hs = ctx->hs;
     HSeedArgs a;
     a.n = ctx->n;
+    a.pos4 = ctx->pos4;
     a.h = ctx->h;
     a.dhdt = ctx->dhdt;
     a.rho = ctx->rho;
@@ -503,7 +522,7 @@ sph_status launch_hseed_infer(sph_ctx *ctx, cudaStream_t st) {
     sph_status s = hseed_alloc(ctx);
     if (s != SPH_OK) return s;
     const int tiles = (ctx->n + kTile - 1) / kTile;
-    k_mlp<0><<<tiles, kTile, kFwdBytes, st>>>(hseed_args(ctx), 0u, 0);
+    k_mlp<0><<<tiles, kTile, kFwdBytes, st>>>(hseed_args(ctx), 0u, 0, nullptr);
     return cuda_status(cudaGetLastError(), "h seed inference");
 }
 
@@ -515,18 +534,39 @@ sph_status launch_hseed_norm(sph_ctx *ctx, cudaStream_t st) {
     return cuda_status(cudaGetLastError(), "h seed normalisation");
 }
 
-sph_status launch_hseed_grad(sph_ctx *ctx, uint32_t it, int batch, uint32_t salt, cudaStream_t st) {
+// Gradients of a minibatch: rows of iteration it (+ the Adam step counter
+// when counted).
+sph_status launch_hseed_grad(sph_ctx *ctx, uint32_t it, bool counted, int batch, uint32_t salt, cudaStream_t st) {
     HSeedArgs a = hseed_args(ctx);
     a.salt = salt;
     const int tiles = (batch + kTile - 1) / kTile;
-    k_mlp<1><<<tiles, kTile, kTrainBytes, st>>>(a, it, batch);
+    k_mlp<1><<<tiles, kTile, kTrainBytes, st>>>(a, it, batch, counted ? ctx->hs.adam_step : nullptr);
     return cuda_status(cudaGetLastError(), "h seed gradient");
 }
 
 sph_status launch_hseed_adam(sph_ctx *ctx, float lr, cudaStream_t st) {
     HSeed &hs = ctx->hs;
-    k_adam<<<(kNParams + 255) / 256, 256, 0, st>>>(hs.params, hs.grads, hs.adam_m, hs.adam_v, ++hs.steps, lr);
+    k_adam<<<1, kAdamThreads, 0, st>>>(hs.params, hs.grads, hs.adam_m, hs.adam_v, hs.adam_step, lr);
     return cuda_status(cudaGetLastError(), "h seed update");
+}
+
+// Standardisation from the recorded pass, then `iterations` Adam steps (the
+// minibatch of step s is drawn by s + 1); stream-ordered, graph-capturable.
+sph_status launch_hseed_steps(sph_ctx *ctx, int iterations, int batch, float lr, cudaStream_t st) {
+    sph_status s = launch_hseed_norm(ctx, st);
+    for (int i = 0; i < iterations && s == SPH_OK; ++i) {
+        s = launch_hseed_grad(ctx, 1u, true, batch, 0x5bd1e995u, st);
+        if (s == SPH_OK) s = launch_hseed_adam(ctx, lr, st);
+    }
+    return s;
+}
+
+bool hseed_online_due(const sph_ctx *ctx) {
+    return ctx->form.h_seed == SPH_HSEED_LEARNED && ctx->hs.online_iters > 0 && ctx->hs.have_data;
+}
+
+sph_status launch_hseed_online(sph_ctx *ctx, cudaStream_t st) {
+    return launch_hseed_steps(ctx, ctx->hs.online_iters, ctx->hs.online_batch, ctx->hs.online_lr, st);
 }
 
 }  // namespace sph
@@ -560,13 +600,14 @@ sph_status sph_hseed_train(sph_ctx *ctx, int32_t iterations, int32_t batch, floa
     }
     cudaSetDevice(ctx->device);
     cudaStream_t st = (cudaStream_t)stream;
-    sph_status s = SPH_OK;
-    if (!ctx->hs.have_norm) s = launch_hseed_norm(ctx, st);
+    // the standardisation follows the recorded pass (the first pass after the
+    // initial conditions has no neighbour counts or dh/dt yet)
+    sph_status s = iterations > 0 ? launch_hseed_steps(ctx, iterations - 1, batch, lr, st) : SPH_OK;
     float last = 0.f;
-    for (int32_t i = 0; i < iterations && s == SPH_OK; ++i) {
-        const bool final = i + 1 == iterations;
-        if (final) cudaMemsetAsync(ctx->hs.loss, 0, sizeof(float), st);
-        s = launch_hseed_grad(ctx, (uint32_t)(ctx->hs.steps + 1), batch, 0x5bd1e995u, st);
+    if (s == SPH_OK && iterations > 0) {
+        // the last step also reports its minibatch loss
+        cudaMemsetAsync(ctx->hs.loss, 0, sizeof(float), st);
+        s = launch_hseed_grad(ctx, 1u, true, batch, 0x5bd1e995u, st);
         if (s == SPH_OK) s = launch_hseed_adam(ctx, lr, st);
     }
     if (s != SPH_OK) return s;
@@ -576,6 +617,25 @@ sph_status sph_hseed_train(sph_ctx *ctx, int32_t iterations, int32_t batch, floa
         if (e != cudaSuccess) return cuda_status(e, "sph_hseed_train");
     }
     if (loss) *loss = last;
+    return SPH_OK;
+}
+
+sph_status sph_hseed_online(sph_ctx *ctx, int32_t iterations, int32_t batch, float lr) {
+    if (!ctx || iterations < 0 || iterations > 4096 || batch < 1 || batch > (1 << 22) || !(lr > 0.f)) {
+        set_error("sph_hseed_online: bad arguments");
+        return SPH_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    if (iterations > 0) {
+        sph_status s = hseed_alloc(ctx);
+        if (s != SPH_OK) return s;
+    }
+    drop_graphs(ctx);
+    ctx->hs.online_iters = iterations;
+    ctx->hs.online_batch = batch;
+    ctx->hs.online_lr = lr;
+    // every density pass records its pairs while the refresh is on
+    ctx->hs.capture = iterations > 0;
     return SPH_OK;
 }
 
@@ -595,7 +655,7 @@ sph_status sph_hseed_gradient(sph_ctx *ctx, int32_t batch, uint32_t salt, float 
     if (s != SPH_OK) return s;
     cudaMemsetAsync(ctx->hs.grads, 0, sizeof(float) * kNParams, st);
     cudaMemsetAsync(ctx->hs.loss, 0, sizeof(float), st);
-    s = launch_hseed_grad(ctx, 0u, batch, salt, st);
+    s = launch_hseed_grad(ctx, 0u, false, batch, salt, st);
     if (s != SPH_OK) return s;
     float l = 0.f;
     cudaError_t e = cudaMemcpyAsync(grads, ctx->hs.grads, sizeof(float) * kNParams, cudaMemcpyDeviceToHost, st);

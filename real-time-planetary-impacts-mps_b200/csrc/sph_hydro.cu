@@ -2181,6 +2181,9 @@ sph_status launch_density(sph_ctx *ctx, cudaStream_t st) {
     a.nn_out = ctx->hs.nn;
     a.stats = ctx->hs.stats;
     sph_status s = SPH_OK;
+    // the learned seed's online refresh, unless a full step ran it ahead
+    if (hseed_online_due(ctx) && !ctx->hs.trained_ahead) s = launch_hseed_online(ctx, st);
+    if (s != SPH_OK) return s;
     if (ctx->hs.stats) cudaMemsetAsync(ctx->hs.stats, 0, sizeof(uint32_t) * 4, st);
     if (ctx->hs.capture) s = launch_hseed_capture(ctx, st);
     if (s == SPH_OK && ctx->form.h_seed == SPH_HSEED_LEARNED) {

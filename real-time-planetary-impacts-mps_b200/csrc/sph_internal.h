@@ -97,18 +97,25 @@ struct HSeed {
     float *norm = nullptr;
     double *norm_part = nullptr;
     float *X = nullptr;     // [n][8] raw features of the captured pass
-    float *y = nullptr;     // [n] targets log(h_converged / h0)
+    float *y = nullptr;     // [n] targets log(h_fix / h0)
     float *h0 = nullptr;    // [n] h at the start of the captured pass
     float *nn = nullptr;    // [n] neighbour count of the last density pass
     float *seed = nullptr;  // [n] predicted starting h
     float *loss = nullptr;  // running loss of a training call
     uint32_t *stats = nullptr;  // density-pass counters: [0] NR iterations, [1] fallbacks, [2] max, [3] particles
-    int steps = 0;          // Adam steps taken
+    uint32_t *adam_step = nullptr;  // device: Adam steps taken (bias correction, sample rows)
     bool have_data = false, have_norm = false, capture = false;
+    // online refresh (sph_hseed_online): Adam steps per full step on the
+    // previous density pass's recorded pairs, run before the next density
+    // pass (beside the tree, sort and gravity passes in a full step)
+    int online_iters = 0, online_batch = 16384;
+    float online_lr = 1e-3f;
+    bool trained_ahead = false;  // this step's refresh is already enqueued
 };
 
 struct HSeedArgs {
     int n;
+    const float4 *pos4;  // (x, y, z, mass)
     const float *h, *dhdt, *rho, *u;
     const int32_t *mat, *nat;
     const uint8_t *active;
@@ -237,7 +244,7 @@ sph_status launch_hseed_capture(sph_ctx *ctx, cudaStream_t st);
 sph_status launch_hseed_targets(sph_ctx *ctx, cudaStream_t st);
 sph_status launch_hseed_infer(sph_ctx *ctx, cudaStream_t st);
 sph_status launch_hseed_norm(sph_ctx *ctx, cudaStream_t st);
-sph_status launch_hseed_grad(sph_ctx *ctx, uint32_t it, int batch, uint32_t salt, cudaStream_t st);
+sph_status launch_hseed_grad(sph_ctx *ctx, uint32_t it, bool counted, int batch, uint32_t salt, cudaStream_t st);
 sph_status launch_hseed_adam(sph_ctx *ctx, float lr, cudaStream_t st);
 
 // sph_gravity_theta.cu
@@ -255,6 +262,10 @@ sph_status launch_tree_build(sph_ctx *ctx, cudaStream_t st);
 // sph_api.cu
 // One full step (tree, sort, gravity, density, acceleration, step) on st.
 sph_status full_step(sph_ctx *ctx, cudaStream_t st);
+// sph_hseed.cu: the online refresh of the learned seed (standardisation and
+// Adam steps on the last recorded pass) on st; whether one is due this step
+bool hseed_online_due(const sph_ctx *ctx);
+sph_status launch_hseed_online(sph_ctx *ctx, cudaStream_t st);
 // Destroy the captured step graphs (sph_step_all's and sph_step_host's):
 // called whenever what they replay changes.
 void drop_graphs(sph_ctx *ctx);

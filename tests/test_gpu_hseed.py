@@ -111,3 +111,41 @@ def test_learned_seed_against_plain_guess(cuda, pkg):
         rel = np.abs(a - b) / b
         print(f"  tight tolerance: converged h max relative difference {rel.max():.2e}")
         assert rel.max() <= 1e-6
+
+
+def test_online_refresh_keeps_the_seed_fresh(cuda, pkg):
+    """Graph-replayed steps with the online refresh (sph_hseed_online): the
+    weights keep changing from replay to replay (the Adam step counter and the
+    minibatches live on the device), and after 12 steps the seeded density
+    passes still take fewer sweeps than the plain start at the same point."""
+    ic = pkg.ic.make_impact(80000, 20000, seed=2)
+    res = {}
+    for online in (False, True):
+        with recorded(pkg, ic, steps=1) as c:
+            for _ in range(2):
+                c.step()
+                c.hseed_train(200, 16384, 1e-3)
+            c.hseed_capture(False)
+            c.set_form(h_seed="learned")
+            if online:
+                c.hseed_online(16, 16384, 1e-3)
+            c.step_all(2)
+            c.synchronize()
+            p0 = c.hseed_params()
+            c.step_all(12)
+            c.synchronize()
+            assert c.health() == 0
+            st = c.hseed_stats()
+            res[online] = (st["sweeps"] / st["particles"], st["fallbacks"] / st["particles"])
+            changed = not np.array_equal(p0, c.hseed_params())
+            assert changed == online
+    with recorded(pkg, ic, steps=1) as c:
+        c.hseed_capture(False)
+        c.step_all(2 + 2 + 12)
+        c.synchronize()
+        st = c.hseed_stats()
+        plain = st["sweeps"] / st["particles"]
+    print(f"\n  sweeps/particle after 16 steps: plain start {plain:.2f}, seed trained once {res[False][0]:.2f} "
+          f"(fallback {res[False][1]:.4f}), refreshed online {res[True][0]:.2f} (fallback {res[True][1]:.4f})")
+    assert res[True][0] < plain
+    assert res[True][1] < 0.02
