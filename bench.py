@@ -66,14 +66,21 @@ PASS_KERNELS = {
 }
 
 
-def launches_per_step(depth: int, chosen: bool) -> int:
-    """Kernels of one step (memsets excluded), counted from the pass structure."""
+def launches_per_step(depth: int, chosen: bool, online_iters: int = 0, seed: bool | None = None) -> int:
+    """Kernels of one step (memsets excluded), counted from the pass structure
+    (matches the ncu launch list: 116 plain, 131 chosen with 8 online Adam
+    steps, at depth 7)."""
     scan = 4  # reduce, blocks, apply, total
     tree = 3 + 3 + 1 + depth * (1 + scan + 1) + 1 + 1 + (depth + 1) + 2 * scan + (depth + 1) + depth
-    sort = 1 + 3 + 1
+    sort = 1 + 3 + 1 + 1                 # hash, 3 passes, cells, units
     gravity = (depth + 1) + 2 if chosen else 2 * (depth + 1)
-    density = 4 + (1 if chosen else 0)   # gather, tile starts, tile pass, deferred pass [, seed]
-    acceleration = 3                     # tile starts, tile pass, deferred pass
+    # gather, tile starts, tile pass, coarse starts, coarse tile pass, deferred pass
+    density = 6
+    if chosen if seed is None else seed:
+        density += 3                     # seed inference, pair capture, targets
+        if online_iters > 0:
+            density += 2 + 2 * online_iters  # standardisation, gradient + Adam per step
+    acceleration = 5                     # tile starts, tile pass, coarse starts, coarse pass, deferred pass
     return tree + sort + gravity + density + acceleration + 1
 
 
@@ -435,7 +442,7 @@ def run_ensemble(args, rank: int, world: int, local: int):
             "e2e": {"value": total * K / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(d2h // max(K, 1)) * world,
                     "path": "sph_ensemble_step(1) + every instance's global time read back, per step"},
-            "gpu_launches": launches_per_step(DEPTH, True) * len(specs) * K,
+            "gpu_launches": launches_per_step(DEPTH, True, seed=False) * len(specs) * K,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -645,7 +652,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "form": "chosen",
                     "path": "sph_step_host (pos64, vel, u, h, rho in and out, pinned), one sync per step"},
-            "gpu_launches": launches_per_step(DEPTH, True) * K,
+            "gpu_launches": launches_per_step(DEPTH, True, args.online_iters) * K,
             "clocks": clocks,
         }
         line.update(extra)
