@@ -462,7 +462,7 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="particle count relative to 1e6 (diagnostics)")
     ap.add_argument("--theta", type=float, default=0.6, help="opening angle of the chosen form's gravity")
     ap.add_argument("--train-iters", type=int, default=600, help="Adam steps after each warm-up step")
-    ap.add_argument("--online-iters", type=int, default=8,
+    ap.add_argument("--online-iters", type=int, default=4,
                     help="Adam steps of the seed's online refresh per step (0: seed trained in warm-up only)")
     ap.add_argument("--drift-steps", type=int, default=100,
                     help="steps of the energy-drift comparison (the 1000-step comparison runs at config 0 in the tests)")
