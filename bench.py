@@ -460,6 +460,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="particle count relative to 1e6 (diagnostics)")
+    ap.add_argument("--no-coarse-tiles", action="store_true",
+                    help="hand particles whose neighbour boxes reach past 3 cells to the per-particle walk")
     ap.add_argument("--theta", type=float, default=0.6, help="opening angle of the chosen form's gravity")
     ap.add_argument("--train-iters", type=int, default=600, help="Adam steps after each warm-up step")
     ap.add_argument("--online-iters", type=int, default=4,
@@ -504,6 +506,8 @@ def main():
 
     # ---- plain form -------------------------------------------------------
     cp = pkg.Compute(ic, max_children_in_leaf=LEAF, max_tree_depth=DEPTH)
+    if args.no_coarse_tiles:
+        cp.set_tiling(coarse=False)
     cp.hseed_capture(True)  # allocates the density-pass counters; records nothing once off
     cp.hseed_capture(False)
     with torch.cuda.stream(stream):
@@ -513,6 +517,8 @@ def main():
     cp.synchronize()
     # ---- chosen form: theta gravity, mixed precision, learned h seed --------
     cc = pkg.Compute(ic, max_children_in_leaf=LEAF, max_tree_depth=DEPTH)
+    if args.no_coarse_tiles:
+        cc.set_tiling(coarse=False)
     cc.set_form(gravity="theta", theta=args.theta, precision="mixed")
     cc.hseed_capture(True)
     train_ms = []
@@ -620,7 +626,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": chosen_ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 positions, time and reductions in the chosen form)",
             "data": "synthetic (seeded two-body impact generator)",
-            "config": {"workload": f"two-body impact N={n} (800k+200k), leaf {LEAF}, depth {DEPTH}",
+            "config": {"workload": f"two-body impact N={n} ({int(N_TARGET * args.scale)}+"
+                                   f"{int(N_IMPACTOR * args.scale)}), leaf {LEAF}, depth {DEPTH}",
                        "form": f"chosen: theta {args.theta} gravity + mixed precision + learned h seed"
                                + (f" (refreshed online, {args.online_iters} Adam steps per step)"
                                   if args.online_iters > 0 else ""),
