@@ -467,7 +467,7 @@ class Compute:
     def clear_health(self):
         self._check(self._lib.sph_clear_health(self._h), "sph_clear_health")
 
-    # ---- checkpoint / resume (the reference has no resume) ----
+    # ---- checkpoint / resume (the reference has no resume) --------------
     CHECKPOINT_FIELDS = ("pos", "vel", "acc", "rho", "u", "mass", "pressure", "h", "grad_term", "sound_speed",
                          "du", "balsara", "dhdt", "grav_norm", "material", "active", "next_active_time",
                          "global_time", "dt")
